@@ -1,0 +1,90 @@
+"""Compile the CUDA library in-tree: adaptflood_b200/libadaptflood.so (sm_100a).
+
+Floating-point flags per translation unit:
+  * af_plain.cu, af_step_f64.cu, af_sim.cu: -fmad=false, so FP64 expressions
+    round exactly as the reference's C++ does on the CPU;
+  * af_step_f32.cu: -use_fast_math (FP32 path: FMA contraction, approximate
+    division/sqrt and SFU exp2/log2 are within its error budget).
+Host code is compiled with -ffp-contract=off for the same reason.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libadaptflood.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
+HOSTCXX = "/usr/bin/g++"
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+          "-Xcompiler", "-ffp-contract=off", "-ccbin", HOSTCXX, "-I", INCLUDE, "-I", CSRC]
+EXACT = ["-fmad=false"]
+FAST = ["-use_fast_math"]
+
+UNITS = [
+    ("af_plain.cu", EXACT),
+    ("af_step_f64.cu", EXACT),
+    ("af_step_f32.cu", FAST),
+    ("af_sim.cu", EXACT),
+]
+HOST_UNITS = ["af_io.cpp"]
+HEADERS = ["af_common.cuh", "af_step.cuh"]
+
+
+def _newer(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("command failed: " + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    return r.stdout + r.stderr
+
+
+def build(verbose: bool = False, ptxas_info: bool = False) -> str:
+    os.makedirs(OBJ, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "adaptflood.h")]
+    jobs = []
+    objs = []
+    for src, flags in UNITS:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src + ".o")
+        objs.append(o)
+        if ptxas_info or _newer(o, [s, __file__] + hdrs):
+            extra = ["-Xptxas", "-v"] if ptxas_info else []
+            jobs.append([NVCC, *ARCH, *COMMON, *flags, *extra, "-c", s, "-o", o])
+    for src in HOST_UNITS:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src + ".o")
+        objs.append(o)
+        if _newer(o, [s, __file__] + hdrs):
+            jobs.append([HOSTCXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off",
+                         "-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o])
+    log = []
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
+        for out in ex.map(_run, jobs):
+            log.append(out)
+    if jobs or not os.path.exists(LIB):
+        log.append(_run([NVCC, *ARCH, "-shared", "-ccbin", HOSTCXX, "-o", LIB, *objs,
+                         "-lcudart", "-lcudadevrt"]))
+    text = "".join(log)
+    if verbose:
+        print(text)
+    return text
+
+
+if __name__ == "__main__":
+    print(build(verbose=False, ptxas_info="--ptxas" in sys.argv) or "up to date")

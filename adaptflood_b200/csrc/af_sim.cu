@@ -1,0 +1,795 @@
+// af_sim.cu -- the simulation layer: device-resident state, forcing tables,
+// special-cell lists, and the CUDA graph that runs the time loop.
+//
+// Memory layout in HBM (per precision T, N = 16 bytes / sizeof(T)):
+//   every array has a front guard of kGuard elements and rows of pitch P,
+//   P >= nsx*OWN + N rounded up to 32 elements, so every 16-byte lane vector
+//   of every strip (halo lanes included) is inside the allocation and aligned;
+//   H[2], DEM: ny rows of cells (column i = cell i)
+//   Qx[2]:     ny rows of x-faces (column i = west face of cell i, i <= nx)
+//   Qy[2]:     ny+1 rows of y-faces (row j = north face of row j)
+// Padding is zero and never read into an owned result.
+//
+// The time loop (src/main.cpp:227 `while (t < sim_time)`) is one graph
+// launch: a begin kernel sets the stop condition, then a conditional WHILE
+// node re-runs the step kernel until its last block clears the condition.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "af_step.cuh"
+
+namespace af {
+
+constexpr int kGuard = 64;
+constexpr int kMassCap = 1 << 16;
+
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+template <typename V>
+static int upload(DevBuf& b, const std::vector<V>& v, cudaStream_t st) {
+  size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(V);
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    cuda_fail(e);
+    return AF_ENOMEM;
+  }
+  if (!v.empty()) AF_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(V),
+                                          cudaMemcpyHostToDevice, st));
+  return AF_OK;
+}
+
+static bool non_decreasing(const double* t, int n) {
+  for (int i = 0; i + 1 < n; i++)
+    if (!(t[i] <= t[i + 1])) return false;
+  for (int i = 0; i < n; i++)
+    if (t[i] != t[i]) return false;
+  return true;
+}
+
+// ------------------------------------------------------------- kernels
+template <typename T>
+__global__ void k_hmax_int(const T* __restrict__ H, const T* __restrict__ Z, int nx, int ny,
+                           int P, double nodata, unsigned long long* acc) {
+  double m = -DBL_MAX;
+  const T nd = T(nodata);
+  long long n = (long long)nx * ny;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    long long j = k / nx, i = k - j * nx;
+    double h = (double)H[j * P + i];
+    if (Z[j * P + i] != nd && h > m) m = h;
+  }
+  m = warp_maxd(m);
+  if ((threadIdx.x & 31) == 0 && m > -DBL_MAX) atomicMax(acc, ord_encode(m));
+}
+
+__global__ void k_ctl_fold_hmax(SimCtl* ctl) {
+  ctl->hmax = ord_decode(ctl->hmax_acc);
+  ctl->hmax_acc = ord_encode(-DBL_MAX);
+}
+
+// Sets the stop condition of one launch: the loop runs while t < t_stop and
+// fewer than max_steps steps have run in this launch.
+__global__ void k_begin(SimCtl* ctl, double t_stop, long long max_steps,
+                        cudaGraphConditionalHandle cond, int use_cond) {
+  ctl->t_stop = t_stop;
+  long long s = ctl->step;
+  ctl->step_stop = (max_steps > (long long)0x3FFFFFFFFFFFFFFFLL - s) ? 0x3FFFFFFFFFFFFFFFLL
+                                                                      : s + max_steps;
+  int done = !(ctl->t < t_stop) || max_steps <= 0;
+  ctl->done = done;
+  ctl->arrive = 0u;
+  if (use_cond) cudaGraphSetConditional(cond, done ? 0u : 1u);
+}
+
+// ComputeVelocity_GPU (src/kernels.cpp:293-351) on the padded layout.
+template <typename T>
+__global__ void k_velocity_int(const T* __restrict__ H, const T* __restrict__ Z,
+                               const T* __restrict__ Qx, const T* __restrict__ Qy, int nx,
+                               int j0, int j1, int P, double dx, double nodata,
+                               double* __restrict__ Vx, double* __restrict__ Vy) {
+  long long n = (long long)nx * (j1 - j0);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    int jr = (int)(k / nx), i = (int)(k - (long long)jr * nx);
+    long long r = (long long)(j0 + jr) * P;
+    double z = (double)Z[r + i], h = (double)H[r + i];
+    if (z == (double)T(nodata) || h < 0.001) {
+      Vx[k] = 0.0;
+      Vy[k] = 0.0;
+      continue;
+    }
+    double hflow = h;
+    if (hflow < 0.001) hflow = 0.001;
+    double ql = (double)Qx[r + i], qr = (double)Qx[r + i + 1];
+    double vl = (fabs(ql) > 1e-10) ? ql / dx / hflow : 0.0;
+    double vr = (fabs(qr) > 1e-10) ? qr / dx / hflow : 0.0;
+    Vx[k] = (fabs(vl) > fabs(vr)) ? vl : vr;
+    double qt = (double)Qy[r + i], qb = (double)Qy[r + P + i];
+    double vt = (fabs(qt) > 1e-10) ? qt / dx / hflow : 0.0;
+    double vb = (fabs(qb) > 1e-10) ? qb / dx / hflow : 0.0;
+    Vy[k] = (fabs(vt) > fabs(vb)) ? vt : vb;
+  }
+}
+
+// Volume and flooded area of the state (src/main.cpp:293-298), fixed order.
+template <typename T>
+__global__ void k_volume_int(const T* __restrict__ H, int nx, int ny, int P, double dA,
+                             double* __restrict__ part) {
+  long long n = (long long)nx * ny;
+  long long chunk = (n + gridDim.x - 1) / gridDim.x;
+  long long lo = blockIdx.x * chunk, hi = min(lo + chunk, n);
+  double s = 0.0, c = 0.0, a = 0.0;
+  for (long long k = lo + threadIdx.x; k < hi; k += blockDim.x) {
+    long long j = k / nx, i = k - j * nx;
+    double h = (double)H[j * P + i];
+    kahan_add(s, c, h * dA);
+    if (h > 0.01) a += dA;
+  }
+  __shared__ double ss[256], sc[256], sa[256];
+  ss[threadIdx.x] = s;
+  sc[threadIdx.x] = c;
+  sa[threadIdx.x] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double S = 0.0, C = 0.0, A = 0.0;
+    for (int k = 0; k < (int)blockDim.x; k++) {
+      kahan_add(S, C, ss[k]);
+      C += sc[k];
+      A += sa[k];
+    }
+    part[3 * blockIdx.x] = S;
+    part[3 * blockIdx.x + 1] = C;
+    part[3 * blockIdx.x + 2] = A;
+  }
+}
+
+// ----------------------------------------------------------- the object
+struct Sim {
+  int device = 0;
+  int prec = AF_PREC_F64;
+  int esize = 8, N = 2;
+  cudaStream_t st = nullptr;
+  af_case_desc c{};
+  int P = 0, nsx = 0, nsy = 0, R = 16, WX = 4;
+  size_t cells_elems = 0, qy_elems = 0;  // allocation sizes (elements, guards included)
+  DevBuf H[2], Qx[2], Qy[2], DEM;
+  DevBuf src_type, src_value, src_off, src_times, src_vals, src_sorted;
+  DevBuf bc_type, bc_value, bc_off, bc_times, bc_vals, bc_sorted;
+  DevBuf rain_times, rain_rates, spec_off, spec;
+  DevBuf ctl, partials, mass_series;
+  SimCtl* pinned_ctl = nullptr;
+  StepParams prm{};
+  dim3 grid, block;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphNode_t begin_node = nullptr;
+  cudaGraphConditionalHandle cond = 0;
+  bool use_cond = false;
+  int n_rain = 0;
+  std::vector<double> rain_t, rain_r;
+
+  ~Sim() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (pinned_ctl) cudaFreeHost(pinned_ctl);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  template <typename T>
+  T* buf(DevBuf& b) const { return static_cast<T*>(b.p) + kGuard; }
+};
+
+static int pick_shape(Sim& s) {
+  // Rows per strip and warps per block by grid size: small grids need many
+  // short strips to fill 148 SMs; large grids amortise the strip prologue.
+  const long long cells = (long long)s.c.nx * s.c.ny;
+  const int own = 30 * s.N;
+  s.nsx = (s.c.nx + own - 1) / own;
+  if (cells <= (1LL << 20)) s.R = 4;
+  else if (cells <= (1LL << 23)) s.R = 8;
+  else if (cells <= (1LL << 25)) s.R = 16;
+  else s.R = 32;
+  s.WX = s.nsx >= 4 ? 4 : (s.nsx >= 2 ? 2 : 1);
+  s.nsy = (s.c.ny + s.R - 1) / s.R;
+  s.grid = dim3((s.nsx + s.WX - 1) / s.WX, s.nsy);
+  s.block = dim3(32 * s.WX);
+  return AF_OK;
+}
+
+static int alloc_field(DevBuf& b, size_t elems, int esize) {
+  cudaError_t e = cudaMalloc(&b.p, elems * esize);
+  if (e != cudaSuccess) {
+    cuda_fail(e);
+    return AF_ENOMEM;
+  }
+  return AF_OK;
+}
+
+// Copies a host FP64 field with `rows` x `width` entries and host pitch
+// `hpitch` into the padded device field (converted to the sim precision).
+static int put_field(Sim& s, DevBuf& b, const double* src, int rows, int width, size_t hpitch) {
+  char* dst = static_cast<char*>(b.p) + (size_t)kGuard * s.esize;
+  if (s.prec == AF_PREC_F64) {
+    AF_CUDA(cudaMemcpy2DAsync(dst, (size_t)s.P * 8, src, hpitch * 8, (size_t)width * 8, rows,
+                              cudaMemcpyHostToDevice, s.st));
+    AF_CUDA(cudaStreamSynchronize(s.st));
+    return AF_OK;
+  }
+  std::vector<float> tmp((size_t)rows * width);
+  for (int j = 0; j < rows; j++)
+    for (int i = 0; i < width; i++) tmp[(size_t)j * width + i] = (float)src[(size_t)j * hpitch + i];
+  AF_CUDA(cudaMemcpy2DAsync(dst, (size_t)s.P * 4, tmp.data(), (size_t)width * 4,
+                            (size_t)width * 4, rows, cudaMemcpyHostToDevice, s.st));
+  AF_CUDA(cudaStreamSynchronize(s.st));
+  return AF_OK;
+}
+
+static int get_field(Sim& s, DevBuf& b, double* dst, int rows, int width, size_t hpitch) {
+  const char* src = static_cast<const char*>(b.p) + (size_t)kGuard * s.esize;
+  if (s.prec == AF_PREC_F64) {
+    AF_CUDA(cudaMemcpy2DAsync(dst, hpitch * 8, src, (size_t)s.P * 8, (size_t)width * 8, rows,
+                              cudaMemcpyDeviceToHost, s.st));
+    AF_CUDA(cudaStreamSynchronize(s.st));
+    return AF_OK;
+  }
+  std::vector<float> tmp((size_t)rows * width);
+  AF_CUDA(cudaMemcpy2DAsync(tmp.data(), (size_t)width * 4, src, (size_t)s.P * 4,
+                            (size_t)width * 4, rows, cudaMemcpyDeviceToHost, s.st));
+  AF_CUDA(cudaStreamSynchronize(s.st));
+  for (int j = 0; j < rows; j++)
+    for (int i = 0; i < width; i++) dst[(size_t)j * hpitch + i] = (double)tmp[(size_t)j * width + i];
+  return AF_OK;
+}
+
+static int refresh_hmax(Sim& s, int parity) {
+  SimCtl* ctl = static_cast<SimCtl*>(s.ctl.p);
+  unsigned grid = grid_for((long long)s.c.nx * s.c.ny, 256, 8);
+  if (s.prec == AF_PREC_F64)
+    k_hmax_int<double><<<grid, 256, 0, s.st>>>(s.buf<double>(s.H[parity]), s.buf<double>(s.DEM),
+                                               s.c.nx, s.c.ny, s.P, s.c.nodata, &ctl->hmax_acc);
+  else
+    k_hmax_int<float><<<grid, 256, 0, s.st>>>(s.buf<float>(s.H[parity]), s.buf<float>(s.DEM),
+                                              s.c.nx, s.c.ny, s.P, s.c.nodata, &ctl->hmax_acc);
+  k_ctl_fold_hmax<<<1, 1, 0, s.st>>>(ctl);
+  AF_CUDA(cudaGetLastError());
+  return AF_OK;
+}
+
+static int read_ctl(Sim& s) {
+  AF_CUDA(cudaMemcpyAsync(s.pinned_ctl, s.ctl.p, sizeof(SimCtl), cudaMemcpyDeviceToHost, s.st));
+  AF_CUDA(cudaStreamSynchronize(s.st));
+  return AF_OK;
+}
+
+static int write_ctl(Sim& s) {
+  AF_CUDA(cudaMemcpyAsync(s.ctl.p, s.pinned_ctl, sizeof(SimCtl), cudaMemcpyHostToDevice, s.st));
+  AF_CUDA(cudaStreamSynchronize(s.st));
+  return AF_OK;
+}
+
+static double first_mass_after(double t, double mass_int) {
+  if (!(mass_int > 0.0)) return 0.0;
+  double nm = mass_int;  // src/main.cpp:200, advanced as :303 does
+  while (nm <= t) nm += mass_int;
+  return nm;
+}
+
+static int build_graph(Sim& s) {
+  AF_CUDA(cudaGraphCreate(&s.graph, 0));
+  SimCtl* ctl = static_cast<SimCtl*>(s.ctl.p);
+  s.use_cond = cudaGraphConditionalHandleCreate(&s.cond, s.graph, 0, 0) == cudaSuccess;
+  if (!s.use_cond) {
+    cudaGetLastError();
+    cudaGraphDestroy(s.graph);
+    s.graph = nullptr;
+    return AF_OK;  // fall back to host-driven launches
+  }
+  s.prm.cond = s.cond;
+  s.prm.use_cond = 1;
+  double t_stop = 0.0;
+  long long max_steps = 0;
+  int use = 1;
+  void* bargs[] = {&ctl, &t_stop, &max_steps, &s.cond, &use};
+  cudaKernelNodeParams kb{};
+  kb.func = (void*)&k_begin;
+  kb.gridDim = dim3(1);
+  kb.blockDim = dim3(1);
+  kb.kernelParams = bargs;
+  AF_CUDA(cudaGraphAddKernelNode(&s.begin_node, s.graph, nullptr, 0, &kb));
+
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = s.cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  AF_CUDA(cudaGraphAddNode(&cnode, s.graph, &s.begin_node, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+
+  void* sargs[] = {&s.prm};
+  cudaKernelNodeParams ks{};
+  ks.func = const_cast<void*>(s.prec == AF_PREC_F64 ? step_kernel_f64(s.WX) : step_kernel_f32(s.WX));
+  ks.gridDim = s.grid;
+  ks.blockDim = s.block;
+  ks.kernelParams = sargs;
+  cudaGraphNode_t snode;
+  AF_CUDA(cudaGraphAddKernelNode(&snode, body, nullptr, 0, &ks));
+  AF_CUDA(cudaGraphInstantiate(&s.exec, s.graph, 0));
+  return AF_OK;
+}
+
+static int create(const af_case_desc* c, const af_forcing_desc* f, const double* dem,
+                  const double* h0, int precision, int device, Sim** out) {
+  if (!c || !f || !dem || !out) return AF_EINVAL;
+  if (precision != AF_PREC_F64 && precision != AF_PREC_F32) return AF_EINVAL;
+  if (c->nx < 2 || c->ny < 2) return AF_EINVAL;
+  if (!(c->dx > 0.0) || c->theta != 1.0) return AF_EINVAL;
+  if ((long long)(c->nx + 1) * (c->ny + 1) > 0x7FFFFFFFLL) return AF_ERANGE;
+  if (f->n_flow < 0 || f->n_other < 0 || f->n_rain < 0) return AF_EINVAL;
+  const long long ncell = (long long)c->nx * c->ny;
+  for (int k = 0; k < f->n_flow; k++)
+    if (f->flow_idx[k] < 0 || f->flow_idx[k] >= ncell) return AF_ERANGE;
+  for (int k = 0; k < f->n_other; k++)
+    if (f->other_idx[k] < 0 || f->other_idx[k] >= ncell) return AF_ERANGE;
+
+  std::unique_ptr<Sim> s(new Sim());
+  s->device = device;
+  s->prec = precision;
+  s->esize = precision == AF_PREC_F64 ? 8 : 4;
+  s->N = 16 / s->esize;
+  s->c = *c;
+  AF_CUDA(cudaSetDevice(device));
+  AF_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  AF_CUDA(cudaMallocHost(&s->pinned_ctl, sizeof(SimCtl)));
+  pick_shape(*s);
+  const int own = 30 * s->N;
+  int P = s->nsx * own + s->N;
+  P = (P + 31) / 32 * 32;
+  s->P = P;
+  const int nx = c->nx, ny = c->ny;
+  s->cells_elems = (size_t)kGuard * 2 + (size_t)ny * P;
+  s->qy_elems = (size_t)kGuard * 2 + (size_t)(ny + 1) * P;
+  for (int b = 0; b < 2; b++) {
+    AF_TRY(alloc_field(s->H[b], s->cells_elems, s->esize));
+    AF_TRY(alloc_field(s->Qx[b], s->cells_elems, s->esize));
+    AF_TRY(alloc_field(s->Qy[b], s->qy_elems, s->esize));
+    AF_CUDA(cudaMemsetAsync(s->H[b].p, 0, s->cells_elems * s->esize, s->st));
+    AF_CUDA(cudaMemsetAsync(s->Qx[b].p, 0, s->cells_elems * s->esize, s->st));
+    AF_CUDA(cudaMemsetAsync(s->Qy[b].p, 0, s->qy_elems * s->esize, s->st));
+  }
+  AF_TRY(alloc_field(s->DEM, s->cells_elems, s->esize));
+  AF_CUDA(cudaMemsetAsync(s->DEM.p, 0, s->cells_elems * s->esize, s->st));
+  AF_TRY(put_field(*s, s->DEM, dem, ny, nx, nx));
+  if (h0) AF_TRY(put_field(*s, s->H[0], h0, ny, nx, nx));
+
+  // ---- point sources, stably sorted by cell (file order kept per cell)
+  std::vector<int> order(f->n_flow);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return f->flow_idx[a] < f->flow_idx[b]; });
+  std::vector<int> st_type, st_off(1, 0);
+  std::vector<double> st_value, st_times, st_vals;
+  std::vector<unsigned char> st_sorted;
+  for (int k : order) {
+    st_type.push_back(f->flow_type[k]);
+    st_value.push_back(f->flow_value[k]);
+    int n = 0;
+    if (f->flow_type[k] == AF_BC_QVAR) {
+      int o = f->flow_off[k];
+      n = f->flow_off[k + 1] - o;
+      st_times.insert(st_times.end(), f->flow_times + o, f->flow_times + o + n);
+      st_vals.insert(st_vals.end(), f->flow_vals + o, f->flow_vals + o + n);
+      st_sorted.push_back(non_decreasing(f->flow_times + o, n) ? 1 : 0);
+    } else {
+      st_sorted.push_back(1);
+    }
+    st_off.push_back(st_off.back() + n);
+  }
+  // ---- point depth BCs: the last effective one per cell wins (file order)
+  std::vector<int> bt(f->n_other), bo(f->n_other + 1, 0);
+  std::vector<double> bv(f->n_other), btimes, bvals;
+  std::vector<unsigned char> bsorted(f->n_other);
+  for (int k = 0; k < f->n_other; k++) {
+    bt[k] = f->other_type[k];
+    bv[k] = f->other_value[k];
+    int n = 0;
+    if (bt[k] == AF_BC_HVAR) {
+      int o = f->other_off[k];
+      n = f->other_off[k + 1] - o;
+      btimes.insert(btimes.end(), f->other_times + o, f->other_times + o + n);
+      bvals.insert(bvals.end(), f->other_vals + o, f->other_vals + o + n);
+    }
+    bo[k + 1] = bo[k] + n;
+    bsorted[k] = non_decreasing(btimes.data() + bo[k], n) ? 1 : 0;
+  }
+  // ---- special cells
+  struct Ent {
+    long long key;
+    SpecCell e;
+  };
+  std::vector<Ent> ents;
+  {
+    size_t k = 0;
+    std::vector<std::pair<int, int>> last_bc;  // (cell, bc)
+    for (int b = 0; b < f->n_other; b++)
+      if (bt[b] == 1 || bt[b] == 2 || bt[b] == 3) last_bc.push_back({f->other_idx[b], b});
+    std::stable_sort(last_bc.begin(), last_bc.end(),
+                     [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+                       return a.first < b.first;
+                     });
+    std::vector<std::pair<int, int>> bc_of;  // cell -> last bc
+    for (size_t q = 0; q < last_bc.size(); q++)
+      if (q + 1 == last_bc.size() || last_bc[q + 1].first != last_bc[q].first)
+        bc_of.push_back(last_bc[q]);
+    size_t qb = 0;
+    auto emit = [&](int cell, int s0, int s1, int bc) {
+      SpecCell e{};
+      e.row = cell / nx;
+      e.col = cell % nx;
+      e.s0 = s0;
+      e.s1 = s1;
+      e.bc = bc;
+      int sx = e.col / own, sy = e.row / s->R;
+      long long strip = (long long)sy * s->nsx + sx;
+      ents.push_back({(strip << 40) | ((long long)e.row << 20) | 0, e});
+    };
+    // merge the sorted source cells with the sorted bc cells
+    while (k < order.size() || qb < bc_of.size()) {
+      int cs = k < order.size() ? f->flow_idx[order[k]] : 0x7FFFFFFF;
+      int cbc = qb < bc_of.size() ? bc_of[qb].first : 0x7FFFFFFF;
+      int cell = std::min(cs, cbc);
+      int s0 = (int)k;
+      while (k < order.size() && f->flow_idx[order[k]] == cell) k++;
+      int bc = -1;
+      if (cbc == cell) {
+        bc = bc_of[qb].second;
+        qb++;
+      }
+      emit(cell, s0, (int)k, bc);
+    }
+  }
+  std::stable_sort(ents.begin(), ents.end(), [](const Ent& a, const Ent& b) {
+    if (a.key != b.key) return a.key < b.key;
+    return a.e.col < b.e.col;
+  });
+  const long long nstrips = (long long)s->nsx * s->nsy;
+  std::vector<int> soff(nstrips + 1, 0);
+  std::vector<SpecCell> spec;
+  for (auto& e : ents) {
+    soff[(e.key >> 40) + 1]++;
+    spec.push_back(e.e);
+  }
+  for (long long q = 0; q < nstrips; q++) soff[q + 1] += soff[q];
+
+  AF_TRY(upload(s->src_type, st_type, s->st));
+  AF_TRY(upload(s->src_value, st_value, s->st));
+  AF_TRY(upload(s->src_off, st_off, s->st));
+  AF_TRY(upload(s->src_times, st_times, s->st));
+  AF_TRY(upload(s->src_vals, st_vals, s->st));
+  AF_TRY(upload(s->src_sorted, st_sorted, s->st));
+  AF_TRY(upload(s->bc_type, bt, s->st));
+  AF_TRY(upload(s->bc_value, bv, s->st));
+  AF_TRY(upload(s->bc_off, bo, s->st));
+  AF_TRY(upload(s->bc_times, btimes, s->st));
+  AF_TRY(upload(s->bc_vals, bvals, s->st));
+  AF_TRY(upload(s->bc_sorted, bsorted, s->st));
+  s->rain_t.assign(f->rain_times, f->rain_times + f->n_rain);
+  s->rain_r.assign(f->rain_rates, f->rain_rates + f->n_rain);
+  s->n_rain = f->n_rain;
+  AF_TRY(upload(s->rain_times, s->rain_t, s->st));
+  AF_TRY(upload(s->rain_rates, s->rain_r, s->st));
+  AF_TRY(upload(s->spec_off, soff, s->st));
+  AF_TRY(upload(s->spec, spec, s->st));
+  const size_t nblocks = (size_t)s->grid.x * s->grid.y;
+  AF_TRY(alloc_field(s->partials, nblocks * 3 + 3, 8));
+  AF_TRY(alloc_field(s->mass_series, (size_t)kMassCap * 3, 8));
+  AF_TRY(alloc_field(s->ctl, 1, sizeof(SimCtl)));
+
+  SimCtl& h = *s->pinned_ctl;
+  memset(&h, 0, sizeof(SimCtl));
+  h.t = 0.0;
+  h.hmax = -DBL_MAX;
+  h.rain_rate = s->n_rain > 0 ? interp_series(s->rain_t.data(), s->rain_r.data(), s->n_rain, 0.0,
+                                              0.0, non_decreasing(s->rain_t.data(), s->n_rain))
+                              : 0.0;
+  h.next_mass = first_mass_after(0.0, c->mass_int);
+  h.hmax_acc = ord_encode(-DBL_MAX);
+  h.done = 1;
+  h.mass_cap = kMassCap;
+  AF_TRY(write_ctl(*s));
+  AF_TRY(refresh_hmax(*s, 0));
+
+  StepParams& p = s->prm;
+  for (int b = 0; b < 2; b++) {
+    p.H[b] = static_cast<char*>(s->H[b].p) + (size_t)kGuard * s->esize;
+    p.Qx[b] = static_cast<char*>(s->Qx[b].p) + (size_t)kGuard * s->esize;
+    p.Qy[b] = static_cast<char*>(s->Qy[b].p) + (size_t)kGuard * s->esize;
+  }
+  p.DEM = static_cast<char*>(s->DEM.p) + (size_t)kGuard * s->esize;
+  p.nx = nx;
+  p.ny = ny;
+  p.P = P;
+  p.nsx = s->nsx;
+  p.nsy = s->nsy;
+  p.R = s->R;
+  p.dx = c->dx;
+  p.dxinv = 1.0 / c->dx;  // src/kernels.cpp:8
+  p.dA = c->dx * c->dx;   // src/main.cpp:115
+  p.fpn = c->fpn;
+  p.depth_thresh = c->depth_thresh;
+  p.max_hflow = c->max_hflow;
+  p.g = c->g;
+  p.cfl = c->cfl;
+  p.init_tstep = c->init_tstep;
+  p.nodata = c->nodata;
+  p.mass_int = c->mass_int;
+  p.wf = c->west_free;
+  p.ef = c->east_free;
+  p.nf = c->north_free;
+  p.sf = c->south_free;
+  p.src_type = (const int*)s->src_type.p;
+  p.src_value = (const double*)s->src_value.p;
+  p.src_off = (const int*)s->src_off.p;
+  p.src_times = (const double*)s->src_times.p;
+  p.src_vals = (const double*)s->src_vals.p;
+  p.src_sorted = (const unsigned char*)s->src_sorted.p;
+  p.bc_type = (const int*)s->bc_type.p;
+  p.bc_value = (const double*)s->bc_value.p;
+  p.bc_off = (const int*)s->bc_off.p;
+  p.bc_times = (const double*)s->bc_times.p;
+  p.bc_vals = (const double*)s->bc_vals.p;
+  p.bc_sorted = (const unsigned char*)s->bc_sorted.p;
+  p.rain_times = (const double*)s->rain_times.p;
+  p.rain_rates = (const double*)s->rain_rates.p;
+  p.n_rain = s->n_rain;
+  p.rain_sorted = non_decreasing(s->rain_t.data(), s->n_rain) ? 1 : 0;
+  p.spec_off = (const int*)s->spec_off.p;
+  p.spec = (const SpecCell*)s->spec.p;
+  p.ctl = static_cast<SimCtl*>(s->ctl.p);
+  p.partials = static_cast<double*>(s->partials.p);
+  p.mass_series = static_cast<double*>(s->mass_series.p);
+  p.use_cond = 0;
+  AF_TRY(build_graph(*s));
+  AF_CUDA(cudaStreamSynchronize(s->st));
+  *out = s.release();
+  return AF_OK;
+}
+
+static int launch(Sim& s, double t_stop, long long max_steps) {
+  AF_CUDA(cudaSetDevice(s.device));
+  SimCtl* ctl = static_cast<SimCtl*>(s.ctl.p);
+  if (s.use_cond) {
+    int use = 1;
+    void* bargs[] = {&ctl, &t_stop, &max_steps, &s.cond, &use};
+    cudaKernelNodeParams kb{};
+    kb.func = (void*)&k_begin;
+    kb.gridDim = dim3(1);
+    kb.blockDim = dim3(1);
+    kb.kernelParams = bargs;
+    AF_CUDA(cudaGraphExecKernelNodeSetParams(s.exec, s.begin_node, &kb));
+    AF_CUDA(cudaGraphLaunch(s.exec, s.st));
+    return AF_OK;
+  }
+  // Host-driven fallback: launch steps in batches, checking completion.
+  k_begin<<<1, 1, 0, s.st>>>(ctl, t_stop, max_steps, 0, 0);
+  const void* fn = s.prec == AF_PREC_F64 ? step_kernel_f64(s.WX) : step_kernel_f32(s.WX);
+  StepParams p = s.prm;
+  void* args[] = {&p};
+  long long left = max_steps;
+  while (left > 0) {
+    long long batch = left < 64 ? left : 64;
+    for (long long k = 0; k < batch; k++)
+      AF_CUDA(cudaLaunchKernel(fn, s.grid, s.block, args, 0, s.st));
+    left -= batch;
+    AF_TRY(read_ctl(s));
+    if (s.pinned_ctl->done) break;
+  }
+  return AF_OK;
+}
+
+}  // namespace af
+
+using af::Sim;
+
+struct af_sim {
+  Sim* s;
+};
+
+extern "C" {
+
+int af_sim_create(const af_case_desc* c, const af_forcing_desc* f, const double* dem,
+                  const double* h0, int precision, int device, af_sim** out) {
+  if (!out) return AF_EINVAL;
+  Sim* s = nullptr;
+  int rc = af::create(c, f, dem, h0, precision, device, &s);
+  if (rc != AF_OK) return rc;
+  *out = new af_sim{s};
+  return AF_OK;
+}
+
+int af_sim_destroy(af_sim* h) {
+  if (!h) return AF_EINVAL;
+  cudaSetDevice(h->s->device);
+  cudaStreamSynchronize(h->s->st);
+  delete h->s;
+  delete h;
+  return AF_OK;
+}
+
+int af_sim_launch(af_sim* h, double t_stop, int64_t max_steps) {
+  if (!h) return AF_EINVAL;
+  return af::launch(*h->s, t_stop, max_steps);
+}
+
+int af_sim_sync(af_sim* h) {
+  if (!h) return AF_EINVAL;
+  AF_CUDA(cudaStreamSynchronize(h->s->st));
+  return AF_OK;
+}
+
+int af_sim_run(af_sim* h, double t_stop, int64_t max_steps, int64_t* steps_done) {
+  if (!h) return AF_EINVAL;
+  Sim& s = *h->s;
+  AF_TRY(af::read_ctl(s));
+  long long before = s.pinned_ctl->step;
+  AF_TRY(af::launch(s, t_stop, max_steps));
+  AF_TRY(af::read_ctl(s));
+  if (steps_done) *steps_done = s.pinned_ctl->step - before;
+  return AF_OK;
+}
+
+int af_sim_status(af_sim* h, double* t, double* dt_last, double* hmax, int64_t* steps) {
+  if (!h) return AF_EINVAL;
+  Sim& s = *h->s;
+  AF_TRY(af::read_ctl(s));
+  if (t) *t = s.pinned_ctl->t;
+  if (dt_last) *dt_last = s.pinned_ctl->dt_last;
+  if (hmax) *hmax = s.pinned_ctl->hmax;
+  if (steps) *steps = s.pinned_ctl->step;
+  return AF_OK;
+}
+
+void* af_sim_stream(af_sim* h) { return h ? (void*)h->s->st : nullptr; }
+
+int af_sim_get_state(af_sim* h, double* H, double* Qx, double* Qy) {
+  if (!h) return AF_EINVAL;
+  Sim& s = *h->s;
+  AF_CUDA(cudaSetDevice(s.device));
+  AF_TRY(af::read_ctl(s));
+  const int par = s.pinned_ctl->parity;
+  const int nx = s.c.nx, ny = s.c.ny;
+  if (H) AF_TRY(af::get_field(s, s.H[par], H, ny, nx, nx));
+  if (Qx) {
+    AF_TRY(af::get_field(s, s.Qx[par], Qx, ny, nx + 1, nx + 1));
+    for (int i = 0; i <= nx; i++) Qx[(size_t)ny * (nx + 1) + i] = 0.0;
+  }
+  if (Qy) {
+    AF_TRY(af::get_field(s, s.Qy[par], Qy, ny + 1, nx, nx + 1));
+    for (int j = 0; j <= ny; j++) Qy[(size_t)j * (nx + 1) + nx] = 0.0;
+  }
+  return AF_OK;
+}
+
+int af_sim_set_state(af_sim* h, const double* H, const double* Qx, const double* Qy, double t) {
+  if (!h) return AF_EINVAL;
+  Sim& s = *h->s;
+  AF_CUDA(cudaSetDevice(s.device));
+  AF_TRY(af::read_ctl(s));
+  const int par = s.pinned_ctl->parity;
+  const int nx = s.c.nx, ny = s.c.ny;
+  if (H) AF_TRY(af::put_field(s, s.H[par], H, ny, nx, nx));
+  if (Qx) AF_TRY(af::put_field(s, s.Qx[par], Qx, ny, nx + 1, nx + 1));
+  if (Qy) AF_TRY(af::put_field(s, s.Qy[par], Qy, ny + 1, nx, nx + 1));
+  af::SimCtl& c = *s.pinned_ctl;
+  c.t = t;
+  c.rain_rate = s.n_rain > 0 ? af::interp_series(s.rain_t.data(), s.rain_r.data(), s.n_rain, 0.0,
+                                                 t, af::non_decreasing(s.rain_t.data(), s.n_rain))
+                             : 0.0;
+  c.next_mass = af::first_mass_after(t, s.c.mass_int);
+  c.hmax_acc = af::ord_encode(-DBL_MAX);
+  c.arrive = 0;
+  c.done = 1;
+  AF_TRY(af::write_ctl(s));
+  AF_TRY(af::refresh_hmax(s, par));
+  AF_CUDA(cudaStreamSynchronize(s.st));
+  return AF_OK;
+}
+
+int af_sim_velocity(af_sim* h, double* Vx, double* Vy) {
+  if (!h || !Vx || !Vy) return AF_EINVAL;
+  Sim& s = *h->s;
+  AF_CUDA(cudaSetDevice(s.device));
+  AF_TRY(af::read_ctl(s));
+  const int par = s.pinned_ctl->parity;
+  const int nx = s.c.nx, ny = s.c.ny;
+  const int rows_per = std::max(1, (int)((64LL << 20) / (16LL * nx)));
+  af::DevBuf tmp;
+  AF_TRY(af::alloc_field(tmp, (size_t)2 * rows_per * nx, 8));
+  double* dvx = static_cast<double*>(tmp.p);
+  double* dvy = dvx + (size_t)rows_per * nx;
+  for (int j0 = 0; j0 < ny; j0 += rows_per) {
+    int j1 = std::min(ny, j0 + rows_per);
+    long long n = (long long)(j1 - j0) * nx;
+    unsigned g = af::grid_for(n, 256, 8);
+    if (s.prec == AF_PREC_F64)
+      af::k_velocity_int<double><<<g, 256, 0, s.st>>>(
+          s.buf<double>(s.H[par]), s.buf<double>(s.DEM), s.buf<double>(s.Qx[par]),
+          s.buf<double>(s.Qy[par]), nx, j0, j1, s.P, s.c.dx, s.c.nodata, dvx, dvy);
+    else
+      af::k_velocity_int<float><<<g, 256, 0, s.st>>>(
+          s.buf<float>(s.H[par]), s.buf<float>(s.DEM), s.buf<float>(s.Qx[par]),
+          s.buf<float>(s.Qy[par]), nx, j0, j1, s.P, s.c.dx, s.c.nodata, dvx, dvy);
+    AF_CUDA(cudaGetLastError());
+    AF_CUDA(cudaMemcpyAsync(Vx + (size_t)j0 * nx, dvx, n * 8, cudaMemcpyDeviceToHost, s.st));
+    AF_CUDA(cudaMemcpyAsync(Vy + (size_t)j0 * nx, dvy, n * 8, cudaMemcpyDeviceToHost, s.st));
+  }
+  AF_CUDA(cudaStreamSynchronize(s.st));
+  return AF_OK;
+}
+
+int af_sim_volume(af_sim* h, double* vol, double* area) {
+  if (!h || !vol || !area) return AF_EINVAL;
+  Sim& s = *h->s;
+  AF_CUDA(cudaSetDevice(s.device));
+  AF_TRY(af::read_ctl(s));
+  const int par = s.pinned_ctl->parity;
+  const int nb = af::kSMs * 4;
+  af::DevBuf part;
+  AF_TRY(af::alloc_field(part, (size_t)nb * 3, 8));
+  double dA = s.c.dx * s.c.dx;
+  if (s.prec == AF_PREC_F64)
+    af::k_volume_int<double><<<nb, 256, 0, s.st>>>(s.buf<double>(s.H[par]), s.c.nx, s.c.ny, s.P,
+                                                   dA, static_cast<double*>(part.p));
+  else
+    af::k_volume_int<float><<<nb, 256, 0, s.st>>>(s.buf<float>(s.H[par]), s.c.nx, s.c.ny, s.P,
+                                                  dA, static_cast<double*>(part.p));
+  AF_CUDA(cudaGetLastError());
+  std::vector<double> hp((size_t)nb * 3);
+  AF_CUDA(cudaMemcpyAsync(hp.data(), part.p, hp.size() * 8, cudaMemcpyDeviceToHost, s.st));
+  AF_CUDA(cudaStreamSynchronize(s.st));
+  double S = 0.0, C = 0.0, A = 0.0;
+  for (int b = 0; b < nb; b++) {
+    double x = hp[3 * b];
+    double t = S + x;
+    if (fabs(S) >= fabs(x)) C += (S - t) + x;
+    else C += (x - t) + S;
+    S = t;
+    C += hp[3 * b + 1];
+    A += hp[3 * b + 2];
+  }
+  *vol = S + C;
+  *area = A;
+  return AF_OK;
+}
+
+int af_sim_mass_series(af_sim* h, double* t, double* vol, double* area, int cap, int* n) {
+  if (!h || !n || cap < 0) return AF_EINVAL;
+  Sim& s = *h->s;
+  AF_TRY(af::read_ctl(s));
+  int cnt = std::min(s.pinned_ctl->mass_count, cap);
+  std::vector<double> buf((size_t)std::max(cnt, 1) * 3);
+  if (cnt > 0) {
+    AF_CUDA(cudaMemcpyAsync(buf.data(), s.mass_series.p, (size_t)cnt * 24, cudaMemcpyDeviceToHost,
+                            s.st));
+    AF_CUDA(cudaStreamSynchronize(s.st));
+  }
+  for (int k = 0; k < cnt; k++) {
+    if (t) t[k] = buf[3 * k];
+    if (vol) vol[k] = buf[3 * k + 1];
+    if (area) area[k] = buf[3 * k + 2];
+  }
+  *n = s.pinned_ctl->mass_count;
+  return AF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,314 @@
+"""Throughput benchmark of the local-inertial time step (cell-updates/s).
+
+Workload (the large single plain run): an 8192 x 8192 grid at 5 m with the
+seeded DEM generator, 4096 QVAR triangular hydrographs at wet-prone cells,
+piecewise 0-50 mm/h rain, an HVAR sinusoidal edge depth and FREE edges,
+started at t = 1800 s from a flooded state (a 25 mm film on every cell and the
+channel filled to 2 m) so that every face is wet.  A step is one time step of
+the whole grid: fluxes, edges, sources, rain, depth update, point BCs and the
+Hmax reduction that sets the next dt.
+
+Our arm times K steps of the fused kernel (one CUDA-graph launch, CUDA events
+on the simulation's stream) in FP32 (the headline `value`) and FP64, reports
+the HBM roofline of the step kernel, the end-to-end rate through the public
+C ABI with host buffers, and the reference's own CPU code timed on a bounded
+sample of the same workload.  `--impl reference` runs the reference's CPU code
+alone (oracle/_ref, built from the reference sources against the Kokkos-API
+shim), on this host's cores.
+
+N > 1 (torchrun): every rank runs an independent replica of the workload
+(scaling "weak"; the time step needs no data exchange between replicas).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from adaptflood_b200 import forcing as fc  # noqa: E402
+from adaptflood_b200 import scenarios as sc  # noqa: E402
+
+BYTES_PER_CELL = {"f32": 28, "f64": 56}  # read H, DEM, Qx, Qy; write H', Qx', Qy'
+T_START = 1800.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=8192)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0,
+                    help="budget of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(size: int):
+    case = sc.config2(n=size)
+    case.h0 = sc.wet_start(case)
+    return case, fc.pack(case)
+
+
+def describe(size: int):
+    return {"workload": f"C2 large plain run {size}x{size} dx=5m, 4096 QVAR sources, rain, "
+                        f"HVAR edge, FREE N/S/E; flooded start at t={T_START:.0f}s",
+            "cells": size * size, "start_t_s": T_START,
+            "l2": "inputs larger than L2 (state >= 1.9 GB vs 126 MB L2)",
+            "parallelism": "replicas"}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            self.proc.wait()
+            self.fh.close()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return None
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                try:
+                    rows.append((float(parts[0]), float(parts[1]), parts[3:7]))
+                except ValueError:
+                    pass
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for _, _, r in rows for k in range(4) if r[k] == "Active"})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": rows[0][1],
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference(case, forcing, h0, seconds: float, max_steps: int):
+    """The reference's own code (oracle/_ref) on this host's cores: as many
+    steps of the same workload as fit in `seconds` (after one warm-up step)."""
+    from oracle import oracle as orc
+    if not orc.ref_available():
+        return None
+    r = orc.RefSim.from_case(case, forcing)
+    F = (case.nx + 1) * (case.ny + 1)
+    z = np.zeros(F)
+    r.set_state(h0.ravel(), z, z, T_START)
+    r.run(1e30, max_steps=1)
+    n = 0
+    t0 = time.perf_counter()
+    while n < max_steps:
+        r.run(1e30, max_steps=1)
+        n += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    el = time.perf_counter() - t0
+    r.close()
+    return {"value": case.cells * n / el, "unit": "cell-updates/s",
+            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+            "kind": "reference", "steps": n, "seconds": el,
+            "sample": f"{n} steps of the same {case.nx}x{case.ny} workload from the same start "
+                      f"state (after 1 warm-up step), reference src/kernels.cpp + main.cpp loop "
+                      f"compiled -O2 -fopenmp against the Kokkos-API shim"}
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    case, forcing = workload(args.size)
+    res = cpu_reference(case, forcing, case.h0, seconds=max(30.0, args.cpu_seconds),
+                        max_steps=max(1, args.steps))
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built here"}))
+        return
+    ms = res["seconds"] * 1e3 / res["steps"]
+    print(json.dumps({
+        "impl": "reference", "metric": "cell-updates/s", "value": res["value"],
+        "unit": "cell-updates/s", "n_gpus": 0, "steps": res["steps"], "warmup": 1,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": describe(args.size),
+        "cpu_baseline": {"value": res["value"], "unit": "cell-updates/s", "cores": res["cores"],
+                         "kind": "reference", "sample": res["sample"]},
+        "e2e": {"value": res["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
+
+
+def time_fused(case, forcing, precision, steps, warmup, device, dist=None):
+    """K fused steps as one graph launch, CUDA events on the sim's stream."""
+    import torch
+    from adaptflood_b200.sim import Simulation
+    F = (case.nx + 1) * (case.ny + 1)
+    zero = np.zeros(F)
+    s = Simulation(case, precision, device=device, forcing=forcing)
+    s.set_state(case.h0, zero, zero, T_START)
+    s.run(1e30, max_steps=warmup)
+    stream = torch.cuda.ExternalStream(s.stream, device=device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    e0.record(stream)
+    s.launch(1e30, steps)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = e0.elapsed_time(e1)
+    t, dt, hmax, n = s.status()
+    s.close()
+    return ms, {"t_end": t, "dt_last": dt, "hmax": hmax}
+
+
+def time_e2e(case, forcing, precision, steps, device):
+    """The public C ABI end to end with host buffers: af_sim_create from host
+    arrays (DEM, start state, forcing: H2D), the K steps, af_sim_get_state
+    (H, Qx, Qy: D2H)."""
+    import torch
+    from adaptflood_b200.sim import Simulation
+    F = (case.nx + 1) * (case.ny + 1)
+    zero = np.zeros(F)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    s = Simulation(case, precision, device=device, forcing=forcing)
+    s.set_state(case.h0, zero, zero, T_START)
+    s.run(1e30, max_steps=steps)
+    st = s.state()
+    el = time.perf_counter() - t0
+    s.close()
+    es = 4 if precision == "f32" else 8
+    h2d = case.cells * 8 * 2 + 2 * F * 8 + sum(a.nbytes for a in forcing.__dict__.values())
+    d2h = st["H"].nbytes + st["Qx"].nbytes + st["Qy"].nbytes
+    del es
+    return case.cells * steps / el, h2d // steps, d2h // steps
+
+
+def traffic_per_cell(kernel_key: str):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        v = d.get(kernel_key)
+        return None if v is None else float(v)
+    return None
+
+
+def run_ours(args, rank: int, world: int):
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        dist = dist_mod
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    case, forcing = workload(args.size)
+    peak, peak_kind = measured_peak()
+
+    with Clocks(local) as clk:
+        ms32, info32 = time_fused(case, forcing, "f32", args.steps, args.warmup, local, dist)
+    ms64, info64 = time_fused(case, forcing, "f64", args.steps, args.warmup, local, dist)
+    if dist is not None:
+        t = torch.tensor([ms32, ms64], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms32, ms64 = float(t[0]), float(t[1])
+    cells = case.cells
+    value = cells * args.steps * world / (ms32 / 1e3)
+    value64 = cells * args.steps * world / (ms64 / 1e3)
+    step_ms32 = ms32 / args.steps
+    step_ms64 = ms64 / args.steps
+    ach32 = BYTES_PER_CELL["f32"] * cells / (step_ms32 / 1e3) / 1e9
+    ach64 = BYTES_PER_CELL["f64"] * cells / (step_ms64 / 1e3) / 1e9
+    tr32 = traffic_per_cell("k_step_f32")
+    tr64 = traffic_per_cell("k_step_f64")
+    e2e_v, h2d, d2h = time_e2e(case, forcing, "f32", args.steps, local)
+    if dist is not None:
+        t = torch.tensor([e2e_v], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        e2e_v = float(t[0]) * world
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference(case, forcing, case.h0, args.cpu_seconds, 10_000)
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": step_ms32, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": describe(args.size),
+            "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
+                         "frac": ach32 / peak, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_cell": BYTES_PER_CELL["f32"],
+                         "traffic": None if tr32 is None else tr32 * cells,
+                         "kernel": "k_step<float> (fused step)"},
+            "fp64": {"value": value64, "ms_per_step": step_ms64, "dtype": "f64",
+                     "roofline": {"achieved": ach64, "peak": peak, "frac": ach64 / peak,
+                                  "unit": "GB/s",
+                                  "traffic": None if tr64 is None else tr64 * cells},
+                     "fp32_over_fp64": value / value64},
+            "e2e": {"value": e2e_v, "unit": "cell-updates/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h),
+                    "path": "af_sim_create from host arrays + K steps + af_sim_get_state"},
+            "gpu_launches": args.steps + 1,
+            "clocks": clk.summary(),
+            "state_after": {"f32": info32, "f64": info64},
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,216 @@
+/* adaptflood.h -- C ABI of the B200-native AdaptFlood local-inertial time step.
+ *
+ * Two layers share this header:
+ *
+ * 1. The drop-in layer (af_update_qs ... af_fill).  One entry point per
+ *    function of the reference's src/kernels.hpp plus the three pieces of
+ *    device work that src/main.cpp does inline.  Arguments keep the
+ *    reference's names, order and meaning; arrays are DEVICE pointers in the
+ *    reference's layout:
+ *        cells  c(i,j) = i + j*xsz                 xsz*ysz entries
+ *        faces  f(i,j) = i + j*(xsz+1)             (xsz+1)*(ysz+1) entries
+ *    (Qx(i,j) = west face of cell (i,j), Qy(i,j) = north face; row 0 north.)
+ *    Every call enqueues on `stream` (a cudaStream_t; NULL = legacy default
+ *    stream) and waits for it before returning, as each reference function
+ *    ends in Kokkos::fence().  The reference's functions return void and abort
+ *    on error; these return AF_OK or a negative AF_E* code.
+ *
+ * 2. The simulation layer (af_sim_*): one fused, graph-launched kernel per
+ *    time step with device-resident dt, time and hydrograph interpolation, in
+ *    FP64 (results within 1e-9 m of the reference) or FP32 state with FP64
+ *    time, interpolation and volume accumulation.
+ *
+ * Point boundaries: the reference's src/main.cpp:256-260 scatter and
+ * src/kernels.cpp:261-274 overwrite run one thread per boundary and race when
+ * two boundaries share a cell.  Here both are deterministic and equal to the
+ * sequential file-order result: sources on one cell accumulate in file order,
+ * and of several depth BCs on one cell the last in file order wins.
+ */
+#ifndef ADAPTFLOOD_H
+#define ADAPTFLOOD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------------- errors */
+#define AF_OK 0
+#define AF_EINVAL (-1)  /* null pointer, negative size, unsupported shape      */
+#define AF_ERANGE (-2)  /* grid beyond int32 indexing, or an index off the grid */
+#define AF_ECUDA (-3)   /* CUDA runtime error (see af_last_cuda_error)         */
+#define AF_ENOMEM (-4)  /* device or host allocation failed                     */
+#define AF_EIO (-5)     /* an input file is missing or malformed                */
+#define AF_ESTATE (-6)  /* the device reported a bad state (e.g. step overflow) */
+
+const char* af_strerror(int code);
+/* The last CUDA error string seen by this library on the calling thread. */
+const char* af_last_cuda_error(void);
+int af_version(void);
+
+/* Boundary types (src/types.hpp:41-48) and the device point-BC codes
+ * (src/main.cpp:187-189). */
+enum { AF_BC_CLOSED = 0, AF_BC_FREE = 1, AF_BC_HFIX = 2, AF_BC_HVAR = 3,
+       AF_BC_QFIX = 4, AF_BC_QVAR = 5 };
+
+/* ===================================================== 1. drop-in layer == */
+
+/* Replaces UpdateQs_GPU (src/kernels.hpp:8-9, src/kernels.cpp:6-19):
+ * Qxold = Qx*(1/dx), Qyold = Qy*(1/dx) over all (xsz+1)*(ysz+1) faces. */
+int af_update_qs(const double* Qx, const double* Qy, double* Qxold, double* Qyold, int xsz,
+                 int ysz, double dx, void* stream);
+
+/* Replaces FloodplainQ_GPU (src/kernels.hpp:12-16, src/kernels.cpp:22-146):
+ * Hmax over valid cells -> *Tstep = cfl*dx/sqrt(g*Hmax) (or InitTstep when
+ * Hmax <= DepthThresh), then the interior x- and y-face fluxes.  *Tstep is a
+ * HOST pointer, written before return.  dy, dhlin, Qlimfact and dA are
+ * accepted and unused, as in the reference. */
+int af_floodplain_q(const double* H, const double* DEM, double* Qx, double* Qy,
+                    const double* Qxold, const double* Qyold, int xsz, int ysz, double dx,
+                    double dy, double FPn, double DepthThresh, double MaxHflow, double dhlin,
+                    double* Tstep, double Qlimfact, double dA, double cfl, double g,
+                    double InitTstep, double theta, double nodata, void* stream);
+
+/* Replaces BCs_GPU (src/kernels.hpp:19-21, src/kernels.cpp:149-256): edge
+ * faces, FREE outflow or CLOSED (0).  dt is accepted and unused.  A grid one
+ * column wide with west_free set is rejected (AF_EINVAL): the reference reads
+ * past the grid there. */
+int af_bcs(double* Qx, double* Qy, const double* H, const double* DEM, int xsz, int ysz,
+           double dx, double g, double dt, double nodata, int west_free, int east_free,
+           int north_free, int south_free, void* stream);
+
+/* Replaces ApplyPointBCs_GPU (src/kernels.hpp:24-25, src/kernels.cpp:259-277):
+ * type 1 (FREE) sets H = 0, types 2/3 (HFIX/HVAR) set H = value; other types
+ * do nothing.  An index outside [0, ncells) is skipped and the call returns
+ * AF_ERANGE.  ncols, dx, dA, Tstep are accepted and unused, as in the
+ * reference; ncells is the grid's cell count (added for the bounds check). */
+int af_apply_point_bcs(double* H, const int* bc_idx, const int* bc_type, const double* bc_value,
+                       int num_bcs, int ncols, double dx, double dA, double Tstep, int ncells,
+                       void* stream);
+
+/* Replaces UpdateH_GPU (src/kernels.hpp:28, src/kernels.cpp:280-290). */
+int af_update_h(double* H, const double* Qx, const double* Qy, int xsz, int ysz, double dA,
+                double Tstep, void* stream);
+
+/* Replaces ComputeVelocity_GPU (src/kernels.hpp:31-33, src/kernels.cpp:293-351). */
+int af_compute_velocity(double* Vx, double* Vy, const double* H, const double* DEM,
+                        const double* Qx, const double* Qy, int xsz, int ysz, double dx,
+                        double nodata, void* stream);
+
+/* Replaces Rainfall_GPU (src/kernels.hpp:36-37, src/kernels.cpp:354-367). */
+int af_rainfall(double* H, const double* DEM, int xsz, int ysz, double rain_rate, double Tstep,
+                double nodata, void* stream);
+
+/* Replaces the inline AddFlowBCs scatter of src/main.cpp:256-260:
+ * H(idx) = max(H(idx) + ps_flow, 0) per source, where the caller forms
+ * ps_flow = q*dx*Tstep/dA as src/main.cpp:253 does.  Indices outside
+ * [0, ncells) are skipped and the call returns AF_ERANGE. */
+int af_add_point_sources(double* H, const int* ps_idx, const double* ps_flow, int num,
+                         int ncells, void* stream);
+
+/* Replaces the inline Vol/Area reductions of src/main.cpp:293-298:
+ * *vol = sum H*dA, *area = sum of dA over H > 0.01 (HOST outputs).  The sum
+ * is formed in a fixed order, so repeated calls agree bit for bit. */
+int af_volume_area(const double* H, int64_t n, double dA, double* vol, double* area,
+                   void* stream);
+
+/* Replaces the inline Init* fills of src/main.cpp:156-160. */
+int af_fill(double* x, int64_t n, double value, void* stream);
+
+/* ================================================== 2. simulation layer == */
+
+enum { AF_PREC_F64 = 0, AF_PREC_F32 = 1 };
+
+/* Grid and scalar parameters of one case (src/main.cpp:115-124). */
+typedef struct af_case_desc {
+  int nx, ny;            /* ncols, nrows                                     */
+  double dx;             /* cellsize; dy = dx and dA = dx*dx as in the reference */
+  double nodata;         /* DEM nodata value                                  */
+  double fpn;            /* Manning n (par key fpfric)                        */
+  double depth_thresh;   /* par key depth_thresh                              */
+  double cfl;            /* par key cfl                                       */
+  double init_tstep;     /* par key initial_tstep                             */
+  double g;              /* 9.81 in the reference                             */
+  double max_hflow;      /* 10.0 in the reference                             */
+  double theta;          /* 1.0 in the reference                              */
+  int west_free, east_free, north_free, south_free;
+  double mass_int;       /* volume/area report interval (s); <= 0: never      */
+} af_case_desc;
+
+/* Point boundaries and rain, HOST arrays (copied at create time).  Flow
+ * sources keep file order with type AF_BC_QFIX/AF_BC_QVAR; other point BCs
+ * keep file order with device codes 1/2/3 (FREE/HFIX/HVAR).  Hydrographs are
+ * CSR: entries off[k]..off[k+1] of times/vals; an empty series means the
+ * fixed value (src/io.cpp:300).  Rain: n_rain == 0 disables rainfall. */
+typedef struct af_forcing_desc {
+  int n_flow;
+  const int* flow_idx;
+  const int* flow_type;
+  const double* flow_value;
+  const int* flow_off;
+  const double* flow_times;
+  const double* flow_vals;
+  int n_other;
+  const int* other_idx;
+  const int* other_type;
+  const double* other_value;
+  const int* other_off;
+  const double* other_times;
+  const double* other_vals;
+  int n_rain;
+  const double* rain_times;
+  const double* rain_rates;
+} af_forcing_desc;
+
+typedef struct af_sim af_sim;
+
+/* Creates a device-resident simulation on `device` from HOST arrays: dem
+ * (nx*ny, reference layout) and optional initial depth h0 (NULL = zeros, as
+ * src/main.cpp:156).  precision is AF_PREC_F64 or AF_PREC_F32. */
+int af_sim_create(const af_case_desc* c, const af_forcing_desc* f, const double* dem,
+                  const double* h0, int precision, int device, af_sim** out);
+int af_sim_destroy(af_sim* s);
+
+/* Enqueues steps while t < t_stop and fewer than max_steps steps have run in
+ * this call (the loop test of src/main.cpp:227), without waiting. */
+int af_sim_launch(af_sim* s, double t_stop, int64_t max_steps);
+/* Waits for the enqueued steps. */
+int af_sim_sync(af_sim* s);
+/* af_sim_launch + af_sim_sync; *steps_done (optional) gets the step count. */
+int af_sim_run(af_sim* s, double t_stop, int64_t max_steps, int64_t* steps_done);
+/* Time, last dt, current Hmax and total steps (after a sync). */
+int af_sim_status(af_sim* s, double* t, double* dt_last, double* hmax, int64_t* steps);
+/* The device stream the simulation runs on (a cudaStream_t). */
+void* af_sim_stream(af_sim* s);
+
+/* State in the reference layout, HOST arrays, FP64: H (nx*ny), Qx and Qy
+ * ((nx+1)*(ny+1), including the never-written corner slots as 0).  Any
+ * pointer may be NULL. */
+int af_sim_get_state(af_sim* s, double* H, double* Qx, double* Qy);
+int af_sim_set_state(af_sim* s, const double* H, const double* Qx, const double* Qy, double t);
+/* Velocity of the current state (ComputeVelocity_GPU semantics), HOST. */
+int af_sim_velocity(af_sim* s, double* Vx, double* Vy);
+/* Volume and flooded area of the current state (FP64 accumulation). */
+int af_sim_volume(af_sim* s, double* vol, double* area);
+/* The mass-report series recorded at each mass_int crossing
+ * (src/main.cpp:291-304): up to cap entries of (t, vol, area). */
+int af_sim_mass_series(af_sim* s, double* t, double* vol, double* area, int cap, int* n);
+
+/* ============================================== 3. input files (host) == */
+
+/* A case parsed from a .par file and the files it names, with the
+ * reference's parsing rules (src/io.cpp:9-296). */
+typedef struct af_scenario af_scenario;
+
+int af_scenario_load(const char* parfile, af_scenario** out);
+void af_scenario_free(af_scenario* sc);
+/* Views into the parsed case (valid until af_scenario_free).  par[0..2] =
+ * sim_time, save_int, mass_int; geo[0..2] = xll, yll, cellsize. */
+int af_scenario_get(const af_scenario* sc, af_case_desc* c, af_forcing_desc* f,
+                    const double** dem, double* par, double* geo);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ADAPTFLOOD_H */

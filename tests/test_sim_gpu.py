@@ -1,0 +1,177 @@
+"""GPU parity of the fused time step (af_sim_*): whole runs against the
+reference's golden outputs and against the oracle on larger cases that cross
+many strips, plus the FP32 path against the FP64 oracle.
+
+Tolerances: FP64 depth and velocity within 1e-9 m (m/s) of the reference;
+step counts and end times equal.  FP32: max depth error <= 1e-3 m and
+relative volume error <= 1e-6 against FP64.
+"""
+import numpy as np
+import pytest
+
+from _util import golden_names, load_golden
+from adaptflood_b200 import forcing as fc
+from adaptflood_b200 import scenarios as sc
+from adaptflood_b200.sim import Simulation
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+DEPTH_TOL = 1e-9
+FP32_DEPTH_TOL = 1e-3
+FP32_MASS_TOL = 1e-6
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fused_fp64_matches_reference(cuda, name):
+    case, f, exp = load_golden(name)
+    with Simulation(case, "f64", forcing=f) as s:
+        n = s.run(case.sim_time)
+        t, _, _, steps = s.status()
+        st = s.state(velocity=True)
+    assert n == int(exp["steps"]) == steps
+    assert abs(t - float(exp["t_end"])) <= 1e-9 * t
+    assert np.max(np.abs(st["H"] - exp["H"])) <= DEPTH_TOL
+    assert np.max(np.abs(st["Vx"] - exp["Vx"])) <= DEPTH_TOL
+    assert np.max(np.abs(st["Vy"] - exp["Vy"])) <= DEPTH_TOL
+    scale = max(1.0, float(np.max(np.abs(exp["Qx"]))), float(np.max(np.abs(exp["Qy"]))))
+    assert np.max(np.abs(st["Qx"] - exp["Qx"])) <= 1e-9 * scale
+    assert np.max(np.abs(st["Qy"] - exp["Qy"])) <= 1e-9 * scale
+
+
+def _strip_edge_case(nx, ny, seed, R_edges=(4, 8, 16, 32), **kw):
+    """A case with sources and depth BCs placed on strip boundaries (columns
+    around multiples of 60 and 120, rows around multiples of the strip height)."""
+    c = sc.small_case(nx, ny, seed=seed, sim_time=kw.pop("sim_time", 400.0), n_qfix=0, n_qvar=0,
+                      **kw)
+    cols = sorted({x for m in (60, 120) for k in range(1, nx // m + 1)
+                   for x in (m * k - 1, m * k, m * k + 1) if x < nx} | {0, 1, nx - 1})
+    rows = sorted({y for r in R_edges for k in range(1, ny // r + 1)
+                   for y in (r * k - 1, r * k) if y < ny} | {0, ny - 1})
+    rng = np.random.default_rng(seed)
+    for n in range(24):
+        i, j = int(rng.choice(cols)), int(rng.choice(rows))
+        if n % 3 == 0:
+            c.points.append(sc.PointBC(sc.QFIX, i, j, value=float(rng.uniform(0.3, 2.0))))
+        elif n % 3 == 1:
+            tt, vv = sc.triangular_hydrograph(float(rng.uniform(0.3, 2.0)), 60.0, 20.0)
+            c.points.append(sc.PointBC(sc.QVAR, i, j, name=f"e{n}", times=tt, values=vv))
+        else:
+            c.points.append(sc.PointBC(sc.HFIX if n % 2 else sc.FREE, i, j, value=0.4))
+    return c
+
+
+@pytest.mark.parametrize("nx,ny,seed,kw", [
+    (131, 77, 21, dict(rain=True)),
+    (250, 203, 22, dict(free=(1, 0, 1, 1), nodata_block=True, n_hvar=2)),
+    (61, 300, 23, dict(free=(0, 1, 0, 1), h0=True)),
+])
+def test_fused_fp64_matches_oracle_across_strips(cuda, nx, ny, seed, kw):
+    case = _strip_edge_case(nx, ny, seed, **kw)
+    f = fc.pack(case)
+    o = orc.OracleSim(case, f)
+    dts = o.run(case.sim_time, record_dt=True)
+    ref = o.state(velocity=True)
+    with Simulation(case, "f64", forcing=f) as s:
+        n = s.run(case.sim_time)
+        st = s.state(velocity=True)
+    assert n == len(dts)
+    for k in ("H", "Vx", "Vy"):
+        assert np.max(np.abs(st[k] - ref[k])) <= DEPTH_TOL, k
+
+
+def test_run_in_pieces_is_bit_identical(cuda):
+    case, f, exp = load_golden("closed_rain_points")
+    with Simulation(case, "f64", forcing=f) as a, Simulation(case, "f64", forcing=f) as b:
+        a.run(case.sim_time)
+        for t_stop in (13.0, 13.0, 77.7, 150.0):
+            b.run(t_stop)
+        b.run(1e30, max_steps=5)
+        b.run(case.sim_time)
+        sa, sb = a.state(), b.state()
+        assert a.status() == b.status()
+    for k in sa:
+        np.testing.assert_array_equal(sa[k], sb[k])
+
+
+def test_state_round_trip_and_resume(cuda):
+    case, f, _ = load_golden("west_north_reservoir")
+    o = orc.OracleSim(case, f)
+    o.run(100.0)
+    mid = o.state()
+    t_mid = o.t
+    o.run(case.sim_time)
+    ref = o.state()
+    with Simulation(case, "f64", forcing=f) as s:
+        s.set_state(mid["H"], mid["Qx"], mid["Qy"], t_mid)
+        got = s.state()
+        np.testing.assert_array_equal(got["H"], mid["H"])
+        np.testing.assert_array_equal(got["Qx"], mid["Qx"])
+        np.testing.assert_array_equal(got["Qy"], mid["Qy"])
+        s.run(case.sim_time)
+        st = s.state()
+    assert np.max(np.abs(st["H"] - ref["H"])) <= DEPTH_TOL
+
+
+def test_mass_series_matches_reference_reports(cuda):
+    case, f, exp = load_golden("centre_source")
+    o = orc.OracleSim(case, f)
+    want = []
+    next_mass = case.mass_int
+    while o.t < case.sim_time:  # src/main.cpp:291-304
+        o.run(1e30, max_steps=1)
+        if o.t >= next_mass:
+            H = o.state(velocity=False)["H"]
+            want.append((o.t, float(np.sum(H) * case.dx * case.dx),
+                         float(np.count_nonzero(H > 0.01)) * case.dx * case.dx))
+            next_mass += case.mass_int
+    with Simulation(case, "f64", forcing=f) as s:
+        s.run(case.sim_time)
+        t, v, a = s.mass_series()
+        vol_now, area_now = s.volume()
+    assert len(t) == len(want) > 0
+    for k, (tw, vw, aw) in enumerate(want):
+        assert abs(t[k] - tw) <= 1e-9 * tw
+        assert abs(v[k] - vw) <= 1e-9 * max(vw, 1.0)
+        assert a[k] == aw
+    assert abs(vol_now - float(exp["vol"])) <= 1e-9 * float(exp["vol"])
+    assert area_now == float(exp["area"])
+
+
+@pytest.mark.parametrize("name", ["closed_rain_points", "centre_source"])
+def test_fp32_within_tolerance_of_fp64(cuda, name):
+    case, f, exp = load_golden(name)
+    with Simulation(case, "f32", forcing=f) as s:
+        s.run(case.sim_time)
+        H = s.depth()
+        vol32, _ = s.volume()
+    err = np.max(np.abs(H - exp["H"]))
+    rel_mass = abs(vol32 - float(exp["vol"])) / float(exp["vol"])
+    assert err <= FP32_DEPTH_TOL, err
+    assert rel_mass <= FP32_MASS_TOL, rel_mass
+
+
+def test_fp32_larger_case(cuda):
+    case = _strip_edge_case(240, 180, 31, rain=True, sim_time=600.0)
+    f = fc.pack(case)
+    o = orc.OracleSim(case, f)
+    o.run(case.sim_time)
+    H64 = o.state(velocity=False)["H"]
+    vol64 = float(np.sum(H64)) * case.dx * case.dx
+    with Simulation(case, "f32", forcing=f) as s:
+        s.run(case.sim_time)
+        H = s.depth()
+        vol32, _ = s.volume()
+    assert np.max(np.abs(H - H64)) <= FP32_DEPTH_TOL
+    assert abs(vol32 - vol64) / vol64 <= FP32_MASS_TOL
+
+
+def test_loaded_par_runs_like_generated_case(cuda, tmp_path):
+    from adaptflood_b200.sim import load_par
+    case, f, exp = load_golden("free_sources")
+    par = case.write(str(tmp_path))
+    c2, f2 = load_par(par)
+    with Simulation(c2, "f64", forcing=f2) as s:
+        s.run(c2.sim_time)
+        H = s.depth()
+    assert np.max(np.abs(H - exp["H"])) <= DEPTH_TOL
