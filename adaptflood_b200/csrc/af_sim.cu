@@ -634,7 +634,8 @@ int af_sim_launch(af_sim* h, double t_stop, int64_t max_steps) {
 int af_sim_sync(af_sim* h) {
   if (!h) return AF_EINVAL;
   AF_CUDA(cudaStreamSynchronize(h->s->st));
-  return AF_OK;
+  AF_TRY(af::read_ctl(*h->s));
+  return h->s->pinned_ctl->status ? AF_ESTATE : AF_OK;
 }
 
 int af_sim_run(af_sim* h, double t_stop, int64_t max_steps, int64_t* steps_done) {
@@ -645,7 +646,7 @@ int af_sim_run(af_sim* h, double t_stop, int64_t max_steps, int64_t* steps_done)
   AF_TRY(af::launch(s, t_stop, max_steps));
   AF_TRY(af::read_ctl(s));
   if (steps_done) *steps_done = s.pinned_ctl->step - before;
-  return AF_OK;
+  return s.pinned_ctl->status ? AF_ESTATE : AF_OK;
 }
 
 int af_sim_status(af_sim* h, double* t, double* dt_last, double* hmax, int64_t* steps) {

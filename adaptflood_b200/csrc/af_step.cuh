@@ -569,7 +569,11 @@ __global__ void __launch_bounds__(32 * WX) k_step(const StepParams p) {
     ctl->rain_rate = p.n_rain > 0 ? interp_series(p.rain_times, p.rain_rates, p.n_rain, 0.0, t_new,
                                                   p.rain_sorted != 0)
                                   : 0.0;
-    const int done = !(t_new < ctl->t_stop) || step_new >= ctl->step_stop;
+    // A non-positive or non-finite dt (a diverged state) would stall time:
+    // stop the loop and report it instead.
+    const bool bad = !(dt > 0.0) || !(t_new < 1.0e300) || !(hmax == hmax);
+    if (bad) ctl->status = 1;
+    const int done = bad || !(t_new < ctl->t_stop) || step_new >= ctl->step_stop;
     ctl->done = done;
     ctl->arrive = 0u;
     __threadfence();

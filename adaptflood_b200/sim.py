@@ -90,13 +90,13 @@ class Simulation:
         self.close()
 
     # ------------------------------------------------------------- stepping
-    def run(self, t_stop: float, max_steps: int = 1 << 62) -> int:
+    def run(self, t_stop: float, max_steps: int = 10_000_000) -> int:
         n = C.c_int64()
         _lib.check(self.lib.af_sim_run(self.h, float(t_stop), int(max_steps), C.byref(n)),
                    "af_sim_run")
         return n.value
 
-    def launch(self, t_stop: float, max_steps: int = 1 << 62) -> None:
+    def launch(self, t_stop: float, max_steps: int = 10_000_000) -> None:
         _lib.check(self.lib.af_sim_launch(self.h, float(t_stop), int(max_steps)), "af_sim_launch")
 
     def sync(self) -> None:
