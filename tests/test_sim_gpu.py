@@ -18,6 +18,9 @@ from oracle import oracle as orc
 pytestmark = pytest.mark.gpu
 
 DEPTH_TOL = 1e-9
+# Velocity V = Q/dx/h divides the few-ulp pow differences in Q by depths down
+# to 1 mm; over hundreds of steps this reaches a few 1e-9 m/s.
+VEL_TOL = 5e-9
 FP32_DEPTH_TOL = 1e-3
 FP32_MASS_TOL = 1e-6
 
@@ -32,8 +35,8 @@ def test_fused_fp64_matches_reference(cuda, name):
     assert n == int(exp["steps"]) == steps
     assert abs(t - float(exp["t_end"])) <= 1e-9 * t
     assert np.max(np.abs(st["H"] - exp["H"])) <= DEPTH_TOL
-    assert np.max(np.abs(st["Vx"] - exp["Vx"])) <= DEPTH_TOL
-    assert np.max(np.abs(st["Vy"] - exp["Vy"])) <= DEPTH_TOL
+    assert np.max(np.abs(st["Vx"] - exp["Vx"])) <= VEL_TOL
+    assert np.max(np.abs(st["Vy"] - exp["Vy"])) <= VEL_TOL
     scale = max(1.0, float(np.max(np.abs(exp["Qx"]))), float(np.max(np.abs(exp["Qy"]))))
     assert np.max(np.abs(st["Qx"] - exp["Qx"])) <= 1e-9 * scale
     assert np.max(np.abs(st["Qy"] - exp["Qy"])) <= 1e-9 * scale
@@ -76,8 +79,9 @@ def test_fused_fp64_matches_oracle_across_strips(cuda, nx, ny, seed, kw):
         n = s.run(case.sim_time)
         st = s.state(velocity=True)
     assert n == len(dts)
-    for k in ("H", "Vx", "Vy"):
-        assert np.max(np.abs(st[k] - ref[k])) <= DEPTH_TOL, k
+    assert np.max(np.abs(st["H"] - ref["H"])) <= DEPTH_TOL
+    for k in ("Vx", "Vy"):
+        assert np.max(np.abs(st[k] - ref[k])) <= VEL_TOL, k
 
 
 def test_run_in_pieces_is_bit_identical(cuda):
@@ -168,10 +172,76 @@ def test_fp32_larger_case(cuda):
 
 def test_loaded_par_runs_like_generated_case(cuda, tmp_path):
     from adaptflood_b200.sim import load_par
-    case, f, exp = load_golden("free_sources")
+    _, _, exp = load_golden("free_sources")
+    # the generator call that produced the "free_sources" fixture
+    case = sc.small_case(40, 32, seed=11, sim_time=300.0, n_qfix=1, n_qvar=2)
     par = case.write(str(tmp_path))
     c2, f2 = load_par(par)
     with Simulation(c2, "f64", forcing=f2) as s:
         s.run(c2.sim_time)
         H = s.depth()
     assert np.max(np.abs(H - exp["H"])) <= DEPTH_TOL
+
+
+@pytest.mark.parametrize("nx,ny,seed,kw", [
+    (131, 77, 21, dict(rain=True)),
+    (250, 203, 22, dict(free=(1, 0, 1, 1), nodata_block=True, n_hvar=2)),
+])
+def test_fused_equals_dropin_kernels_bitwise(cuda, nx, ny, seed, kw):
+    """Both GPU paths use CUDA's pow, so the fused kernel -- if it keeps the
+    reference's operation order everywhere -- must equal the drop-in
+    per-function kernels bit for bit, step after step."""
+    import torch
+    from adaptflood_b200 import kernels as K
+    case = _strip_edge_case(nx, ny, seed, sim_time=150.0, **kw)
+    f = fc.pack(case)
+    dx, dA = case.dx, case.dx * case.dx
+    F = (nx + 1) * (ny + 1)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    H = dev(case.h0.ravel() if case.h0 is not None else np.zeros(nx * ny))
+    DEM = dev(case.dem.ravel())
+    Qx, Qy, Qxo, Qyo = (torch.zeros(F, dtype=torch.float64, device="cuda") for _ in range(4))
+    o = orc.OracleSim(case, f)  # host-side interpolation only
+    import ctypes as C
+    lib = orc._oracle_lib()
+    lib.afo_interp.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double]
+    interp = lambda tt, vv, fx, t: lib.afo_interp(tt.ctypes.data, vv.ctypes.data, len(tt), fx, t)  # noqa
+    del o
+    with Simulation(case, "f64", forcing=f) as s:
+        t = 0.0
+        for step in range(60):
+            Tstep = K.FloodplainQ_GPU(H, DEM, Qx, Qy, Qxo, Qyo, nx, ny, dx, dx, case.fpn,
+                                      case.depth_thresh, 10.0, 0.01, case.init_tstep, 1.0, dA,
+                                      case.cfl, 9.81, case.init_tstep, 1.0, case.nodata)
+            K.BCs_GPU(Qx, Qy, H, DEM, nx, ny, dx, 9.81, Tstep, case.nodata, case.west_free,
+                      case.east_free, case.north_free, case.south_free)
+            if f.n_flow:
+                flow = np.empty(f.n_flow)
+                for k in range(f.n_flow):
+                    a, b = f.flow_off[k], f.flow_off[k + 1]
+                    v = f.flow_value[k] if f.flow_type[k] == 4 else interp(
+                        f.flow_times[a:b].copy(), f.flow_vals[a:b].copy(), f.flow_value[k], t)
+                    flow[k] = v * dx * Tstep / dA
+                K.AddFlowBCs(H, dev(f.flow_idx.astype(np.int32)), dev(flow), f.n_flow)
+            if f.n_rain:
+                K.Rainfall_GPU(H, DEM, nx, ny, interp(f.rain_times, f.rain_rates, 0.0, t), Tstep,
+                               case.nodata)
+            K.UpdateH_GPU(H, Qx, Qy, nx, ny, dA, Tstep)
+            if f.n_other:
+                val = f.other_value.copy()
+                for b in range(f.n_other):
+                    if f.other_type[b] == 3:
+                        a0, a1 = f.other_off[b], f.other_off[b + 1]
+                        val[b] = interp(f.other_times[a0:a1].copy(), f.other_vals[a0:a1].copy(),
+                                        f.other_value[b], t)
+                K.ApplyPointBCs_GPU(H, dev(f.other_idx.astype(np.int32)),
+                                    dev(f.other_type.astype(np.int32)), dev(val), f.n_other, nx,
+                                    dx, dA, Tstep)
+            K.UpdateQs_GPU(Qx, Qy, Qxo, Qyo, nx, ny, dx)
+            t += Tstep
+            s.run(1e30, max_steps=1)
+            st = s.state()
+            assert s.t == t
+            np.testing.assert_array_equal(st["H"].ravel(), H.cpu().numpy(), err_msg=f"step {step}")
+            np.testing.assert_array_equal(st["Qx"].ravel(), Qx.cpu().numpy())
+            np.testing.assert_array_equal(st["Qy"].ravel(), Qy.cpu().numpy())
