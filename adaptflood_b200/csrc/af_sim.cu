@@ -15,6 +15,7 @@
 // node re-runs the step kernel until its last block clears the condition.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -285,6 +286,11 @@ static double first_mass_after(double t, double mass_int) {
 }
 
 static int build_graph(Sim& s) {
+  // AF_SIM_DIRECT_LAUNCH=1 launches the same step kernel from the host in
+  // batches instead of through the conditional graph: profilers cannot see
+  // kernel nodes inside graphs that contain conditional nodes.
+  const char* direct = getenv("AF_SIM_DIRECT_LAUNCH");
+  if (direct && direct[0] && direct[0] != '0') return AF_OK;
   AF_CUDA(cudaGraphCreate(&s.graph, 0));
   SimCtl* ctl = static_cast<SimCtl*>(s.ctl.p);
   s.use_cond = cudaGraphConditionalHandleCreate(&s.cond, s.graph, 0, 0) == cudaSuccess;

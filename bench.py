@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0,
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", choices=["f32", "f64"], default=None,
+                    help="time one precision only (profiling runs)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     return ap.parse_args()
 
 
@@ -244,6 +247,12 @@ def run_ours(args, rank: int, world: int):
     case, forcing = workload(args.size)
     peak, peak_kind = measured_peak()
 
+    if args.only is not None:
+        ms, info = time_fused(case, forcing, args.only, args.steps, args.warmup, local, dist)
+        if rank == 0:
+            print(json.dumps({"profiling_run": args.only, "ms_per_step": ms / args.steps,
+                              "cells": case.cells, "state_after": info}))
+        return
     with Clocks(local) as clk:
         ms32, info32 = time_fused(case, forcing, "f32", args.steps, args.warmup, local, dist)
     ms64, info64 = time_fused(case, forcing, "f64", args.steps, args.warmup, local, dist)
@@ -260,7 +269,8 @@ def run_ours(args, rank: int, world: int):
     ach64 = BYTES_PER_CELL["f64"] * cells / (step_ms64 / 1e3) / 1e9
     tr32 = traffic_per_cell("k_step_f32")
     tr64 = traffic_per_cell("k_step_f64")
-    e2e_v, h2d, d2h = time_e2e(case, forcing, "f32", args.steps, local)
+    e2e_v, h2d, d2h = (0.0, 0, 0) if args.no_e2e else time_e2e(case, forcing, "f32", args.steps,
+                                                                 local)
     if dist is not None:
         t = torch.tensor([e2e_v], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MIN)
