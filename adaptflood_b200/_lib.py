@@ -66,6 +66,7 @@ _SIGS = {
     "af_compute_velocity": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _d, _d, _vp]),
     "af_rainfall": (_i, [_vp, _vp, _i, _i, _d, _d, _d, _vp]),
     "af_add_point_sources": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
+    "af_add_point_sources_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "af_volume_area": (_i, [_vp, _i64, _d, _vp, _vp, _vp]),
     "af_fill": (_i, [_vp, _i64, _d, _vp]),
     "af_sim_create": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),

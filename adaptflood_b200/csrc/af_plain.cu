@@ -720,3 +720,68 @@ int af_fill(double* x, int64_t n, double value, void* stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free point-source scatter.
+//
+// af_add_point_sources keeps its sort keys in library scratch that it grows
+// with cudaMalloc.  This variant does the same work (same kernels, same
+// result) with its scratch in a fixed file-scope device array instead, for
+// callers that cannot have the library allocate device memory.  The array is
+// part of the loaded module: every GPU that loads the library holds its
+// ~33 KB until the process exits.  All calls share it, so calls whose work
+// overlaps on the GPU (two streams, or two host threads) race; the error
+// word is cleared by every call, and the keys are fully rewritten.
+namespace af {
+namespace {
+
+constexpr int kNoAllocMaxSources = AF_NOALLOC_MAX_SOURCES;
+// 32 words (256 bytes) of header -- the error flag in word 0 -- then the keys.
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[32 + kNoAllocMaxSources];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+
+// The device address of g_noalloc_scratch on the current device.  In host code
+// the symbol names a host-side shadow, not device memory, so the address has
+// to be looked up once per device (with that device current).
+int noalloc_scratch(unsigned long long** out) {
+  int dev = 0;
+  AF_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return AF_EINVAL;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e);
+    g_noalloc_addr[dev] = p;
+  }
+  *out = static_cast<unsigned long long*>(g_noalloc_addr[dev]);
+  return AF_OK;
+}
+
+}  // namespace
+}  // namespace af
+
+extern "C" int af_add_point_sources_noalloc(double* H, const int* ps_idx, const double* ps_flow,
+                                            int num, int ncells, void* stream) {
+  using namespace af;
+  if (num < 0 || ncells < 0) return AF_EINVAL;
+  if (num > kNoAllocMaxSources) return AF_ERANGE;  // nothing launched, H untouched
+  if (num == 0) return AF_OK;
+  if (!H || !ps_idx || !ps_flow) return AF_EINVAL;
+  unsigned long long* scratch = nullptr;
+  AF_TRY(noalloc_scratch(&scratch));
+  int* err = reinterpret_cast<int*>(scratch);
+  unsigned long long* keys = scratch + 32;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  AF_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+  k_point_keys<<<grid_for(num, 256), 256, 0, st>>>(ps_idx, num, ncells, keys, err);
+  if (num > 1) k_sort_small<<<1, 1024, 0, st>>>(keys, num);
+  k_apply_sources<<<grid_for(num, 256), 256, 0, st>>>(H, keys, ps_flow, num);
+  AF_CUDA(cudaGetLastError());
+  int host_err = 0;
+  AF_CUDA(cudaMemcpyAsync(&host_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  AF_CUDA(cudaStreamSynchronize(st));
+  return host_err ? AF_ERANGE : AF_OK;
+}

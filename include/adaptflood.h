@@ -109,6 +109,28 @@ int af_rainfall(double* H, const double* DEM, int xsz, int ysz, double rain_rate
 int af_add_point_sources(double* H, const int* ps_idx, const double* ps_flow, int num,
                          int ncells, void* stream);
 
+/* No counterpart in the reference.  The same scatter as af_add_point_sources,
+ * for callers that cannot let this library allocate device memory: a host
+ * application that hands all device memory to its own pool or arena (so a
+ * library cudaMalloc would fail or fragment it), or one that cannot afford
+ * the device-wide synchronisation a cudaFree implies.  It calls no
+ * cudaMalloc, cudaFree or other allocating routine; its sort keys live in a
+ * fixed device array compiled into the library (about 33 KB on every GPU
+ * that loads it, held until the process exits).
+ *   - num may be at most AF_NOALLOC_MAX_SOURCES; a larger num returns
+ *     AF_ERANGE before anything runs, and H is left unchanged.  Indices off
+ *     the grid are skipped and reported with AF_ERANGE, as in
+ *     af_add_point_sources.
+ *   - The first call on each device looks up the array's device address on
+ *     that device (with it current); make that first call before any stream
+ *     capture.
+ *   - Every call shares the one array: calls whose work overlaps on the GPU
+ *     (concurrent streams or host threads) race and must be serialised by
+ *     the caller.  Each call clears the state it relies on. */
+#define AF_NOALLOC_MAX_SOURCES 4096
+int af_add_point_sources_noalloc(double* H, const int* ps_idx, const double* ps_flow, int num,
+                                 int ncells, void* stream);
+
 /* Replaces the inline Vol/Area reductions of src/main.cpp:293-298:
  * *vol = sum H*dA, *area = sum of dA over H > 0.01 (HOST outputs).  The sum
  * is formed in a fixed order, so repeated calls agree bit for bit. */
