@@ -11,7 +11,9 @@ import os
 import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libadaptflood.so")
+# AF_LIB_PATH selects another build of the same library (e.g. to compare
+# code shapes); by default the in-tree build next to this file is used.
+LIB_PATH = os.environ.get("AF_LIB_PATH") or os.path.join(HERE, "libadaptflood.so")
 
 AF_OK, AF_EINVAL, AF_ERANGE, AF_ECUDA, AF_ENOMEM, AF_EIO, AF_ESTATE = 0, -1, -2, -3, -4, -5, -6
 AF_PREC_F64, AF_PREC_F32 = 0, 1

@@ -54,7 +54,13 @@ def _run(cmd):
     return r.stdout + r.stderr
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> str:
+def build(verbose: bool = False, ptxas_info: bool = False, obj_dir: str = None, lib: str = None,
+          defines=()) -> str:
+    """Compiles the library; obj_dir/lib/defines build an alternative
+    configuration elsewhere (the default is the in-tree library)."""
+    OBJ = obj_dir or globals()["OBJ"]
+    LIB = lib or globals()["LIB"]
+    dflags = [f"-D{d}" for d in defines]
     os.makedirs(OBJ, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "adaptflood.h")]
     jobs = []
@@ -65,7 +71,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         objs.append(o)
         if ptxas_info or _newer(o, [s, __file__] + hdrs):
             extra = ["-Xptxas", "-v"] if ptxas_info else []
-            jobs.append([NVCC, *ARCH, *COMMON, *flags, *extra, "-c", s, "-o", o])
+            jobs.append([NVCC, *ARCH, *COMMON, *flags, *dflags, *extra, "-c", s, "-o", o])
     for src in HOST_UNITS:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ, src + ".o")

@@ -161,7 +161,7 @@ struct Sim {
   int esize = 8, N = 2;
   cudaStream_t st = nullptr;
   af_case_desc c{};
-  int P = 0, nsx = 0, nsy = 0, R = 16, WX = 4;
+  int P = 0, nsx = 0, nsy = 0, R = 16, WY = 4, variant = 0;
   size_t cells_elems = 0, qy_elems = 0;  // allocation sizes (elements, guards included)
   DevBuf H[2], Qx[2], Qy[2], DEM;
   DevBuf src_type, src_value, src_off, src_times, src_vals, src_sorted;
@@ -200,10 +200,30 @@ static int pick_shape(Sim& s) {
   else if (cells <= (1LL << 23)) s.R = 8;
   else if (cells <= (1LL << 25)) s.R = 16;
   else s.R = 32;
-  s.WX = s.nsx >= 4 ? 4 : (s.nsx >= 2 ? 2 : 1);
+  if (const char* r = getenv("AF_SIM_ROWS")) {  // strip height override (tuning sweeps)
+    const int v = atoi(r);
+    if (v >= 1 && v <= 4096) s.R = v;
+  }
   s.nsy = (s.c.ny + s.R - 1) / s.R;
-  s.grid = dim3((s.nsx + s.WX - 1) / s.WX, s.nsy);
-  s.block = dim3(32 * s.WX);
+  s.variant = 0;
+  if (const char* v = getenv("AF_SIM_VARIANT")) {
+    const int k = atoi(v);
+    if (k >= 0 && k < kStepVariants) s.variant = k;
+  }
+  s.WY = kStepVariant[s.variant].wy;
+  // Persistent grid: as many blocks as fit on the GPU at once (a whole number
+  // of blocks per SM), never more than there are tiles.
+  const long long tiles = (long long)s.nsx * ((s.nsy + s.WY - 1) / s.WY);
+  const void* fn = s.prec == AF_PREC_F64 ? step_kernel_f64(s.variant) : step_kernel_f32(s.variant);
+  int per_sm = 0, dev = 0, sms = kSMs;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * s.WY, 0) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long slots = (long long)sms * per_sm;
+  s.grid = dim3((unsigned)(tiles < slots ? tiles : slots));
+  s.block = dim3(32 * s.WY);
   return AF_OK;
 }
 
@@ -324,7 +344,7 @@ static int build_graph(Sim& s) {
 
   void* sargs[] = {&s.prm};
   cudaKernelNodeParams ks{};
-  ks.func = const_cast<void*>(s.prec == AF_PREC_F64 ? step_kernel_f64(s.WX) : step_kernel_f32(s.WX));
+  ks.func = const_cast<void*>(s.prec == AF_PREC_F64 ? step_kernel_f64(s.variant) : step_kernel_f32(s.variant));
   ks.gridDim = s.grid;
   ks.blockDim = s.block;
   ks.kernelParams = sargs;
@@ -588,7 +608,7 @@ static int launch(Sim& s, double t_stop, long long max_steps) {
   }
   // Host-driven fallback: launch steps in batches, checking completion.
   k_begin<<<1, 1, 0, s.st>>>(ctl, t_stop, max_steps, 0, 0);
-  const void* fn = s.prec == AF_PREC_F64 ? step_kernel_f64(s.WX) : step_kernel_f32(s.WX);
+  const void* fn = s.prec == AF_PREC_F64 ? step_kernel_f64(s.variant) : step_kernel_f32(s.variant);
   StepParams p = s.prm;
   void* args[] = {&p};
   long long left = max_steps;

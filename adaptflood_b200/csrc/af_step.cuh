@@ -148,6 +148,7 @@ template <typename T>
 struct Phys {
   T dx, fn, depth_thresh, max_hflow, nodata, gdt;  // gdt = g*dt
   T g;
+  T dxinv, gdt_fn2;  // 1/dx and g*dt*fn*fn (FP32 form only)
 };
 
 // Interior face flux with theta == 1 (src/kernels.cpp:51-92 / :101-142).
@@ -246,17 +247,267 @@ __device__ inline T bc_depth(int b, const StepParams& p, double t) {
                          p.bc_sorted[b] != 0));
 }
 
-template <typename T, int WX>
-__global__ void __launch_bounds__(32 * WX) k_step(const StepParams p) {
+// ------------------------------------------------------------ row faces
+// Interior-formula fluxes of one row for one lane: the west face of each of
+// its N cells (qw) and, when `south`, the south face of each (qs).  Inputs are
+// the lane's cells of rows j (h, z, qxo, qyo) and j+1 (hN, zN, qxoN, qyoN),
+// Qold already formed, and the neighbours from the adjacent lanes (L = the
+// cell west of the first, R = the cell east of the last).  The expensive part
+// runs only in warps that have a wet face, and there without branches, so the
+// faces of a lane overlap in the pipelines.  With theta == 1 the reference's
+// `if (Q*dh < 0)` recomputation (src/kernels.cpp:86-89) yields the same Q
+// (both numerators are equal whenever Q != 0), so it is not repeated.
+
+// FP64: the reference's expressions exactly (src/kernels.cpp:60-84).
+__device__ inline void row_faces(const double (&h)[2], const double (&z)[2], const double (&hN)[2],
+                                 const double (&zN)[2], const double (&qxo)[2],
+                                 const double (&qxoN)[2], const double (&qyo)[2],
+                                 const double (&qyoN)[2], double hL, double zL, double qyoL,
+                                 double qyoNL, double qxoR, double qxoNR, bool south,
+                                 const Phys<double>& ph, double (&qw)[2], double (&qs)[2]) {
+  double Z0[4], H0[4], Z1[4], H1[4], Q0[4], QA[4], QB[4], QC[4], QD[4];
+  // faces 0,1: west faces of cells 0,1; faces 2,3: south faces of cells 0,1
+  Z0[0] = zL;   H0[0] = hL;   Z1[0] = z[0]; H1[0] = h[0];
+  Q0[0] = qxo[0]; QA[0] = qyoL; QB[0] = qyo[0]; QC[0] = qyoNL; QD[0] = qyoN[0];
+  Z0[1] = z[0]; H0[1] = h[0]; Z1[1] = z[1]; H1[1] = h[1];
+  Q0[1] = qxo[1]; QA[1] = qyo[0]; QB[1] = qyo[1]; QC[1] = qyoN[0]; QD[1] = qyoN[1];
+  Z0[2] = z[0]; H0[2] = h[0]; Z1[2] = zN[0]; H1[2] = hN[0];
+  Q0[2] = qyoN[0]; QA[2] = qxo[0]; QB[2] = qxo[1]; QC[2] = qxoN[0]; QD[2] = qxoN[1];
+  Z0[3] = z[1]; H0[3] = h[1]; Z1[3] = zN[1]; H1[3] = hN[1];
+  Q0[3] = qyoN[1]; QA[3] = qxo[1]; QB[3] = qxoR; QC[3] = qxoN[1]; QD[3] = qxoNR;
+  double y0[4], y1[4], hf[4];
+  bool wet[4];
+  bool any = false;
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    y0[f] = Z0[f] + H0[f];
+    y1[f] = Z1[f] + H1[f];
+    double hflow = gmaxT(y0[f], y1[f]) - gmaxT(Z0[f], Z1[f]);
+    hflow = gmaxT(hflow, 0.0);
+    hflow = gminT(hflow, ph.max_hflow);
+    hf[f] = hflow;
+    wet[f] = (f < 2 || south) && !(Z0[f] == ph.nodata || Z1[f] == ph.nodata) &&
+             hflow > ph.depth_thresh;
+    any |= wet[f];
+  }
+  double Q[4] = {0.0, 0.0, 0.0, 0.0};
+  if (__any_sync(0xffffffffu, any)) {
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      const double dh = y0[f] - y1[f];
+      const double Sf = -dh / ph.dx;
+      const double hflow = hf[f];
+      const double qy_avg = (QA[f] + QB[f] + QC[f] + QD[f]) / 4.0;
+      const double qvect = sqrt(Q0[f] * Q0[f] + qy_avg * qy_avg);
+      const double numerator = (Q0[f] + 0.0) - (ph.gdt * hflow * Sf);
+      const double denominator =
+          1.0 + ph.gdt * hflow * ph.fn * ph.fn * fabs(qvect) / pow(hflow, 10.0 / 3.0);
+      const double q = numerator / denominator * ph.dx;
+      Q[f] = wet[f] ? q : 0.0;
+    }
+  }
+  qw[0] = Q[0];
+  qw[1] = Q[1];
+  qs[0] = Q[2];
+  qs[1] = Q[3];
+}
+
+// FP32: the same face law on pairs of faces with Blackwell's packed FP32x2
+// instructions; the friction term is written g*dt*n^2*|q|*hflow^(-7/3), with
+// hflow^(-7/3) = exp2(-7/3 * log2(hflow)) on the special-function unit.
+__device__ inline float2 f2(float a, float b) { return make_float2(a, b); }
+
+__device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float2 q0, float2 qa,
+                               float2 qb, float2 qc, float2 qd, bool enable,
+                               const Phys<float>& ph, bool& any) {
+  const float2 y0 = __fadd2_rn(z0, h0), y1 = __fadd2_rn(z1, h1);
+  const float2 hfx = f2(fmaxf(y0.x, y1.x) - fmaxf(z0.x, z1.x),
+                        fmaxf(y0.y, y1.y) - fmaxf(z0.y, z1.y));
+  const float2 hf = f2(fminf(fmaxf(hfx.x, 0.0f), ph.max_hflow),
+                       fminf(fmaxf(hfx.y, 0.0f), ph.max_hflow));
+  const bool wx = enable && z0.x != ph.nodata && z1.x != ph.nodata && hf.x > ph.depth_thresh;
+  const bool wy = enable && z0.y != ph.nodata && z1.y != ph.nodata && hf.y > ph.depth_thresh;
+  any |= wx | wy;
+  // dh/dx = (y0 - y1)/dx; numerator = q0 - g*dt*hflow*Sf = q0 + g*dt*hflow*dh/dx
+  const float2 s = __fmul2_rn(__ffma2_rn(y1, f2(-1.0f, -1.0f), y0), f2(ph.dxinv, ph.dxinv));
+  const float2 a = __fmul2_rn(f2(ph.gdt, ph.gdt), hf);
+  const float2 num = __ffma2_rn(a, s, q0);
+  const float2 qavg = __fmul2_rn(__fadd2_rn(__fadd2_rn(qa, qb), __fadd2_rn(qc, qd)),
+                                 f2(0.25f, 0.25f));
+  const float2 qv2 = __ffma2_rn(q0, q0, __fmul2_rn(qavg, qavg));
+  const float2 qv = f2(sqrtf(qv2.x), sqrtf(qv2.y));
+  const float2 pw = f2(exp2f(-7.0f / 3.0f * __log2f(hf.x)), exp2f(-7.0f / 3.0f * __log2f(hf.y)));
+  const float2 den = __ffma2_rn(__fmul2_rn(f2(ph.gdt_fn2, ph.gdt_fn2), qv), pw, f2(1.0f, 1.0f));
+  const float2 nd = __fmul2_rn(num, f2(ph.dx, ph.dx));
+  return f2(wx ? __fdividef(nd.x, den.x) : 0.0f, wy ? __fdividef(nd.y, den.y) : 0.0f);
+}
+
+__device__ inline void row_faces(const float (&h)[4], const float (&z)[4], const float (&hN)[4],
+                                 const float (&zN)[4], const float (&qxo)[4],
+                                 const float (&qxoN)[4], const float (&qyo)[4],
+                                 const float (&qyoN)[4], float hL, float zL, float qyoL,
+                                 float qyoNL, float qxoR, float qxoNR, bool south,
+                                 const Phys<float>& ph, float (&qw)[4], float (&qs)[4]) {
+  bool any = false;
+  // west faces: (cell k-1, cell k) for k = 0..3
+  const float2 w01 = flux2(f2(zL, z[0]), f2(hL, h[0]), f2(z[0], z[1]), f2(h[0], h[1]),
+                           f2(qxo[0], qxo[1]), f2(qyoL, qyo[0]), f2(qyo[0], qyo[1]),
+                           f2(qyoNL, qyoN[0]), f2(qyoN[0], qyoN[1]), true, ph, any);
+  const float2 w23 = flux2(f2(z[1], z[2]), f2(h[1], h[2]), f2(z[2], z[3]), f2(h[2], h[3]),
+                           f2(qxo[2], qxo[3]), f2(qyo[1], qyo[2]), f2(qyo[2], qyo[3]),
+                           f2(qyoN[1], qyoN[2]), f2(qyoN[2], qyoN[3]), true, ph, any);
+  // south faces: (cell k row j, cell k row j+1)
+  const float2 s01 = flux2(f2(z[0], z[1]), f2(h[0], h[1]), f2(zN[0], zN[1]), f2(hN[0], hN[1]),
+                           f2(qyoN[0], qyoN[1]), f2(qxo[0], qxo[1]), f2(qxo[1], qxo[2]),
+                           f2(qxoN[0], qxoN[1]), f2(qxoN[1], qxoN[2]), south, ph, any);
+  const float2 s23 = flux2(f2(z[2], z[3]), f2(h[2], h[3]), f2(zN[2], zN[3]), f2(hN[2], hN[3]),
+                           f2(qyoN[2], qyoN[3]), f2(qxo[2], qxo[3]), f2(qxo[3], qxoR),
+                           f2(qxoN[2], qxoN[3]), f2(qxoN[3], qxoNR), south, ph, any);
+  (void)any;
+  qw[0] = w01.x; qw[1] = w01.y; qw[2] = w23.x; qw[3] = w23.y;
+  qs[0] = s01.x; qs[1] = s01.y; qs[2] = s23.x; qs[3] = s23.y;
+}
+
+// ----------------------------------------------------------- row staging
+// Each warp streams its rows through a ring of kStages shared-memory stages.
+// One stage holds, for one grid row, the warp's window of 32 lanes x 16 bytes
+// (512 bytes) of each of H, DEM, Qx and Qy.  Lane 0 fills a stage with bulk
+// copies (cp.async.bulk: the TMA engine's untiled global->shared copy, no
+// multicast) that complete on the stage's mbarrier; the lanes wait on it,
+// read their 16 bytes, and the stage is refilled kStages rows ahead.  Every
+// wait is bounded (kWaitLimit polls); on time-out the warp stops, drains its
+// copies in flight (bounded again) and flags the control block.
+constexpr int kStages = 4;
+// Code-shape knobs of the fused step (compile time): unroll factor of the row
+// loop, and whether x-interior strips get their own copy of the row body
+// without per-column edge tests.
+#ifndef AF_ROW_UNROLL
+#define AF_ROW_UNROLL 1
+#endif
+#ifndef AF_EDGE_SPLIT
+#define AF_EDGE_SPLIT 1
+#endif
+constexpr int kRowUnroll = AF_ROW_UNROLL;
+constexpr int kRowBytes = 512;
+constexpr long long kWaitLimit = 1LL << 22;
+
+__device__ inline uint32_t smem_u32(const void* ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+__device__ inline void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count)
+               : "memory");
+}
+__device__ inline void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ inline void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(b))
+      : "memory");
+}
+__device__ inline bool mbar_try_wait(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, P1;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// True once every lane has seen the phase complete; false after kWaitLimit polls.
+__device__ inline bool mbar_wait_warp(uint64_t* b, uint32_t parity) {
+  for (long long i = 0; i < kWaitLimit; i++) {
+    const bool ok = mbar_try_wait(b, parity);
+    if (__all_sync(0xffffffffu, ok)) return true;
+  }
+  return false;
+}
+__device__ inline void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ inline void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ inline void lds_vec(const unsigned char* p, double (&v)[2]) {
+  const double2 t = *reinterpret_cast<const double2*>(p);
+  v[0] = t.x;
+  v[1] = t.y;
+}
+__device__ inline void lds_vec(const unsigned char* p, float (&v)[4]) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  v[0] = t.x;
+  v[1] = t.y;
+  v[2] = t.z;
+  v[3] = t.w;
+}
+
+template <bool B>
+struct BoolC {
+  static constexpr bool value = B;
+};
+
+// Depth update of a lane's cells: rain (src/kernels.cpp:360-365) then the
+// flux divergence (src/kernels.cpp:286-287).  FP64 keeps the reference's
+// expression; FP32 uses packed FP32x2 with dt/dA folded into one factor.
+__device__ inline void update_cells(double (&hn)[2], const double (&qw)[2], const double (&qe)[2],
+                                    const double (&qn)[2], const double (&qs)[2],
+                                    const double (&z)[2], bool rain_on, double rain_depth,
+                                    double dt, double dA, double /*dt_dA*/, double nodata) {
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    double v = hn[k];
+    if (rain_on && z[k] != nodata) {
+      v = v + rain_depth;
+      if (v < 0.0) v = 0.0;
+    }
+    v = v + dt * (qw[k] - qe[k] + qn[k] - qs[k]) / dA;
+    if (v < 0.0) v = 0.0;
+    hn[k] = v;
+  }
+}
+__device__ inline void update_cells(float (&hn)[4], const float (&qw)[4], const float (&qe)[4],
+                                    const float (&qn)[4], const float (&qs)[4],
+                                    const float (&z)[4], bool rain_on, float rain_depth,
+                                    float /*dt*/, float /*dA*/, float dt_dA, float nodata) {
+  if (rain_on) {
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (z[k] != nodata) hn[k] = fmaxf(hn[k] + rain_depth, 0.0f);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k += 2) {
+    const float2 a = __ffma2_rn(f2(qe[k], qe[k + 1]), f2(-1.0f, -1.0f), f2(qw[k], qw[k + 1]));
+    const float2 b = __ffma2_rn(f2(qs[k], qs[k + 1]), f2(-1.0f, -1.0f), f2(qn[k], qn[k + 1]));
+    const float2 v = __ffma2_rn(f2(dt_dA, dt_dA), __fadd2_rn(a, b), f2(hn[k], hn[k + 1]));
+    hn[k] = fmaxf(v.x, 0.0f);
+    hn[k + 1] = fmaxf(v.y, 0.0f);
+  }
+}
+
+// Persistent grid: block b processes tiles b, b + gridDim.x, ...; a tile is
+// WY strips stacked along y (warp w owns strip sy = tile_y*WY + w of column
+// strip sx).  Warps whose strip lies wholly inside the grid in x take a path
+// without the per-column edge tests.
+template <typename T, int WY, int MINB>
+__global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
   constexpr int N = Lanes<T>::N;
   constexpr int OWN = 30 * N;
+  static_assert(32 * N * sizeof(T) == kRowBytes, "one 16-byte vector per lane");
+  __shared__ __align__(128) unsigned char s_ring[WY][kStages][4][kRowBytes];
+  __shared__ __align__(8) uint64_t s_bar[WY][kStages];
   SimCtl* ctl = p.ctl;
   if (*(volatile int*)&ctl->done) return;
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int sx = blockIdx.x * WX + warp;
-  const int sy = blockIdx.y;
   const int parity = ctl->parity;
   const double t = ctl->t;
   const double hmax_prev = ctl->hmax;
@@ -267,7 +518,7 @@ __global__ void __launch_bounds__(32 * WX) k_step(const StepParams p) {
   const double rate = ctl->rain_rate;
   const bool rain_on = rate > 0.0;  // src/kernels.cpp:356
   const T rain_depth = T(rate * dt);
-  const T dtT = T(dt), dAT = T(p.dA), dxinvT = T(p.dxinv);
+  const T dtT = T(dt), dAT = T(p.dA), dxinvT = T(p.dxinv), dt_dA = T(dt / p.dA);
 
   Phys<T> ph;
   ph.dx = T(p.dx);
@@ -277,216 +528,290 @@ __global__ void __launch_bounds__(32 * WX) k_step(const StepParams p) {
   ph.nodata = T(p.nodata);
   ph.g = T(p.g);
   ph.gdt = T(p.g * dt);  // (g*dt) rounded once, as the reference's left-to-right product does
+  ph.dxinv = T(1.0 / p.dx);
+  ph.gdt_fn2 = T(p.g * dt * p.fpn * p.fpn);
 
   double m_loc = -DBL_MAX, v_loc = 0.0, a_loc = 0.0;
+  bool failed = false;
 
-  if (sx < p.nsx) {
-    const int nx = p.nx, ny = p.ny, P = p.P;
-    const T* __restrict__ H = static_cast<const T*>(p.H[parity]);
-    T* __restrict__ Hn = static_cast<T*>(p.H[parity ^ 1]);
-    const T* __restrict__ Qx = static_cast<const T*>(p.Qx[parity]);
-    T* __restrict__ Qxn = static_cast<T*>(p.Qx[parity ^ 1]);
-    const T* __restrict__ Qy = static_cast<const T*>(p.Qy[parity]);
-    T* __restrict__ Qyn = static_cast<T*>(p.Qy[parity ^ 1]);
-    const T* __restrict__ Z = static_cast<const T*>(p.DEM);
+  const int nx = p.nx, ny = p.ny, P = p.P;
+  const T* __restrict__ H = static_cast<const T*>(p.H[parity]);
+  T* __restrict__ Hn = static_cast<T*>(p.H[parity ^ 1]);
+  const T* __restrict__ Qx = static_cast<const T*>(p.Qx[parity]);
+  T* __restrict__ Qxn = static_cast<T*>(p.Qx[parity ^ 1]);
+  const T* __restrict__ Qy = static_cast<const T*>(p.Qy[parity]);
+  T* __restrict__ Qyn = static_cast<T*>(p.Qy[parity ^ 1]);
+  const T* __restrict__ Z = static_cast<const T*>(p.DEM);
+  uint64_t* bar = s_bar[warp];
+  if (lane == 0) {
+    for (int s = 0; s < kStages; s++) mbar_init(&bar[s], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  int kglob = 0;  // stages this warp has consumed so far (position in its ring)
+  const int tiles_y = (p.nsy + WY - 1) / WY;
+  const int ntiles = p.nsx * tiles_y;
+
+  for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+    const int sx = tile % p.nsx;
+    const int sy = (tile / p.nsx) * WY + warp;
+    if (sy >= p.nsy) continue;
 
     const int x0 = sx * OWN;
-    const int cb = x0 - N + lane * N;  // first column of this lane
+    const int cb = x0 - N + lane * N;          // first column of this lane
+    const long long wcol = (long long)x0 - N;  // first column of the warp's window
     const bool own = lane >= 1 && lane <= 30;
     const int j0 = sy * p.R;
     const int j1 = min(j0 + p.R, ny);
     const int strip = sy * p.nsx + sx;
     int sp = p.spec_off[strip];
     const int sp_end = p.spec_off[strip + 1];
+    // Rows to stream: j0-1 (H, DEM, Qx: the prologue) if j0 > 0, then j0..j1
+    // (all four; row ny only exists for Qy).
+    const int rfirst = j0 > 0 ? j0 - 1 : j0;
+    const int nload = j1 + 1 - rfirst;
+    // Lanes 0..3 each copy one array (H, DEM, Qx, Qy) of row rfirst+k into
+    // stage k; lane 0 also posts the expected byte count.  The prologue row
+    // j0-1 has no Qy; row ny has only Qy.
+    const T* const src_of[4] = {H, Z, Qx, Qy};
+    auto issue = [&](int k) {
+      const int r = rfirst + k;
+      const int slot = (kglob + k) % kStages;
+      const int a_lo = r < ny ? 0 : 3;
+      const int a_hi = r < j0 ? 3 : 4;
+      if (lane == 0) mbar_expect_tx(&bar[slot], (uint32_t)((a_hi - a_lo) * kRowBytes));
+      if (lane >= a_lo && lane < a_hi) {
+        fence_proxy_async();
+        bulk_g2s(&s_ring[warp][slot][lane][0], src_of[lane] + (long long)r * P + wcol, kRowBytes,
+                 &bar[slot]);
+      }
+    };
+    for (int k = 0; k < kStages && k < nload; k++) issue(k);
+    __syncwarp();
+    int kc = 0;  // next stage of this strip to consume
+    auto acquire = [&]() -> const unsigned char* {
+      const int q = kglob + kc;
+      if (!mbar_wait_warp(&bar[q % kStages], (uint32_t)((q / kStages) & 1))) return nullptr;
+      return &s_ring[warp][q % kStages][0][0] + lane * 16;
+    };
+    auto release = [&]() {
+      __syncwarp();
+      if (kc + kStages < nload) issue(kc + kStages);
+      kc++;
+    };
 
     T h[N], z[N], qxo[N], qyo[N], qyn[N];
-    {
-      const long long r = (long long)j0 * P + cb;
-      ld_vec(H + r, h);
-      ld_vec(Z + r, z);
-      ld_vec(Qx + r, qxo);
-      ld_vec(Qy + r, qyo);
-#pragma unroll
-      for (int k = 0; k < N; k++) {
-        qxo[k] = qxo[k] * dxinvT;
-        qyo[k] = qyo[k] * dxinvT;
+    T hp[N], zp[N], qxp[N];
+    if (j0 > 0) {
+      const unsigned char* st = acquire();
+      if (!st) failed = true;
+      if (!failed) {
+        lds_vec(st, hp);
+        lds_vec(st + kRowBytes, zp);
+        lds_vec(st + 2 * kRowBytes, qxp);
+        release();
       }
     }
-    // North faces of row j0.
-    if (j0 == 0) {
-#pragma unroll
-      for (int k = 0; k < N; k++) qyn[k] = p.nf ? out_free(h[k], z[k], T(-1), ph) : T(0);
-      if (own) {
-        if (cb + N <= nx) {
-          st_vec(Qyn + cb, qyn);
-        } else {
-#pragma unroll
-          for (int k = 0; k < N; k++)
-            if (cb + k < nx) Qyn[cb + k] = qyn[k];
-        }
-      }
-    } else {
-      T hp[N], zp[N], qxp[N];
-      const long long r = (long long)(j0 - 1) * P + cb;
-      ld_vec(H + r, hp);
-      ld_vec(Z + r, zp);
-      ld_vec(Qx + r, qxp);
-#pragma unroll
-      for (int k = 0; k < N; k++) qxp[k] = qxp[k] * dxinvT;
-      T qxpR = __shfl_down_sync(0xffffffffu, qxp[0], 1);
-      T qxoR = __shfl_down_sync(0xffffffffu, qxo[0], 1);
-#pragma unroll
-      for (int k = 0; k < N; k++) {
-        T qb = (k < N - 1) ? qxp[k + 1] : qxpR;
-        T qd = (k < N - 1) ? qxo[k + 1] : qxoR;
-        qyn[k] = face_flux(zp[k], hp[k], z[k], h[k], qyo[k], qxp[k], qb, qxo[k], qd, ph);
-      }
-    }
-
-    for (int j = j0; j < j1; j++) {
-      const bool has_next = (j + 1 < ny);
-      T hN[N], zN[N], qxoN[N], qyoN[N];
-      {
-        const long long r = (long long)(j + 1) * P + cb;
-        ld_vec(Qy + r, qyoN);
-        if (has_next) {
-          ld_vec(H + r, hN);
-          ld_vec(Z + r, zN);
-          ld_vec(Qx + r, qxoN);
-        } else {
-#pragma unroll
-          for (int k = 0; k < N; k++) hN[k] = zN[k] = qxoN[k] = T(0);
-        }
+    if (!failed) {
+      const unsigned char* st = acquire();
+      if (!st) failed = true;
+      if (!failed) {
+        lds_vec(st, h);
+        lds_vec(st + kRowBytes, z);
+        lds_vec(st + 2 * kRowBytes, qxo);
+        lds_vec(st + 3 * kRowBytes, qyo);
+        release();
 #pragma unroll
         for (int k = 0; k < N; k++) {
-          qyoN[k] = qyoN[k] * dxinvT;
-          qxoN[k] = qxoN[k] * dxinvT;
+          qxo[k] = qxo[k] * dxinvT;
+          qyo[k] = qyo[k] * dxinvT;
         }
       }
-      // Neighbours across lanes.
-      const T hL = __shfl_up_sync(0xffffffffu, h[N - 1], 1);
-      const T zL = __shfl_up_sync(0xffffffffu, z[N - 1], 1);
-      const T qyoL = __shfl_up_sync(0xffffffffu, qyo[N - 1], 1);
-      const T qyoNL = __shfl_up_sync(0xffffffffu, qyoN[N - 1], 1);
-      const T qxoR = __shfl_down_sync(0xffffffffu, qxo[0], 1);
-      const T qxoNR = __shfl_down_sync(0xffffffffu, qxoN[0], 1);
-
-      // West face of every cell (face c between cells c-1 and c).
-      T qw[N];
+    }
+    if (!failed) {
+      // North faces of row j0.
+      if (j0 == 0) {
 #pragma unroll
-      for (int k = 0; k < N; k++) {
-        const int c = cb + k;
-        if (c == 0) {
-          qw[k] = p.wf ? west_free(h[0], z[0], h[1], z[1], ph) : T(0);
-        } else if (c < nx) {
-          T hl = k ? h[k - 1] : hL;
-          T zl = k ? z[k - 1] : zL;
-          T qa = k ? qyo[k - 1] : qyoL;
-          T qc = k ? qyoN[k - 1] : qyoNL;
-          qw[k] = face_flux(zl, hl, z[k], h[k], qxo[k], qa, qyo[k], qc, qyoN[k], ph);
-        } else {
-          qw[k] = T(0);
-        }
-      }
-      const T qwR = __shfl_down_sync(0xffffffffu, qw[0], 1);
-      // South face of every cell (face row j+1).
-      T qs[N];
-#pragma unroll
-      for (int k = 0; k < N; k++) {
-        if (!has_next) {
-          qs[k] = p.sf ? out_free(h[k], z[k], T(1), ph) : T(0);
-        } else {
-          T qb = (k < N - 1) ? qxo[k + 1] : qxoR;
-          T qd = (k < N - 1) ? qxoN[k + 1] : qxoNR;
-          qs[k] = face_flux(z[k], h[k], zN[k], hN[k], qyoN[k], qxo[k], qb, qxoN[k], qd, ph);
-        }
-      }
-      // Depth update of the owned cells.
-      T hn[N];
-#pragma unroll
-      for (int k = 0; k < N; k++) hn[k] = h[k];
-      const int sp_row = sp;
-      // Point sources (src/main.cpp:245-262), before rain and the update.
-      while (sp < sp_end && p.spec[sp].row == j) {
-        const SpecCell e = p.spec[sp];
+        for (int k = 0; k < N; k++) qyn[k] = p.nf ? out_free(h[k], z[k], T(-1), ph) : T(0);
         if (own) {
+          if (cb + N <= nx) {
+            st_vec(Qyn + cb, qyn);
+          } else {
 #pragma unroll
-          for (int k = 0; k < N; k++)
-            if (cb + k == e.col) hn[k] = apply_sources(hn[k], e, p, t, dt);
+            for (int k = 0; k < N; k++)
+              if (cb + k < nx) Qyn[cb + k] = qyn[k];
+          }
         }
-        sp++;
-      }
-      T qe_last = T(0);
+      } else {
 #pragma unroll
-      for (int k = 0; k < N; k++) {
-        const int c = cb + k;
-        T qe;
-        if (c == nx - 1) qe = p.ef ? out_free(h[k], z[k], T(1), ph) : T(0);
-        else qe = (k < N - 1) ? qw[k + 1] : qwR;
-        if (c == nx - 1) qe_last = qe;
-        T v = hn[k];
-        if (rain_on && z[k] != ph.nodata) {  // src/kernels.cpp:360-365
-          v = v + rain_depth;
-          if (v < T(0)) v = T(0);
-        }
-        v = v + dtT * (qw[k] - qe + qyn[k] - qs[k]) / dAT;  // src/kernels.cpp:286
-        if (v < T(0)) v = T(0);
-        hn[k] = v;
-      }
-      // Point depth BCs (src/kernels.cpp:259-277), after the update.
-      for (int q = sp_row; q < sp; q++) {
-        const SpecCell e = p.spec[q];
-        if (own && e.bc >= 0) {
-          const T v = bc_depth<T>(e.bc, p, t);
+        for (int k = 0; k < N; k++) qxp[k] = qxp[k] * dxinvT;
+        const T qxpR = __shfl_down_sync(0xffffffffu, qxp[0], 1);
+        const T qxoR = __shfl_down_sync(0xffffffffu, qxo[0], 1);
 #pragma unroll
-          for (int k = 0; k < N; k++)
-            if (cb + k == e.col) hn[k] = v;
+        for (int k = 0; k < N; k++) {
+          const T qb = (k < N - 1) ? qxp[k + 1] : qxpR;
+          const T qd = (k < N - 1) ? qxo[k + 1] : qxoR;
+          qyn[k] = face_flux(zp[k], hp[k], z[k], h[k], qyo[k], qxp[k], qb, qxo[k], qd, ph);
         }
       }
-      if (own) {
-        const long long r = (long long)j * P + cb;
-        const long long rs = (long long)(j + 1) * P + cb;
-        if (cb + N <= nx) {
-          st_vec(Hn + r, hn);
-          st_vec(Qxn + r, qw);
-          st_vec(Qyn + rs, qs);
-        } else {
+    }
+
+    auto rows = [&](auto edge_tag) {
+      constexpr bool kEdge = decltype(edge_tag)::value;
+#pragma unroll kRowUnroll
+      for (int j = j0; j < j1; j++) {
+        const bool has_next = (j + 1 < ny);
+        T hN[N], zN[N], qxoN[N], qyoN[N];
+        {
+          const unsigned char* st = acquire();
+          if (!st) {
+            failed = true;
+            return;
+          }
+          lds_vec(st + 3 * kRowBytes, qyoN);
+          if (has_next) {
+            lds_vec(st, hN);
+            lds_vec(st + kRowBytes, zN);
+            lds_vec(st + 2 * kRowBytes, qxoN);
+          } else {
+#pragma unroll
+            for (int k = 0; k < N; k++) hN[k] = zN[k] = qxoN[k] = T(0);
+          }
+          release();
 #pragma unroll
           for (int k = 0; k < N; k++) {
-            if (cb + k < nx) {
-              Hn[r + k] = hn[k];
-              Qxn[r + k] = qw[k];
-              Qyn[rs + k] = qs[k];
+            qyoN[k] = qyoN[k] * dxinvT;
+            qxoN[k] = qxoN[k] * dxinvT;
+          }
+        }
+        // Neighbours across lanes.
+        const T hL = __shfl_up_sync(0xffffffffu, h[N - 1], 1);
+        const T zL = __shfl_up_sync(0xffffffffu, z[N - 1], 1);
+        const T qyoL = __shfl_up_sync(0xffffffffu, qyo[N - 1], 1);
+        const T qyoNL = __shfl_up_sync(0xffffffffu, qyoN[N - 1], 1);
+        const T qxoR = __shfl_down_sync(0xffffffffu, qxo[0], 1);
+        const T qxoNR = __shfl_down_sync(0xffffffffu, qxoN[0], 1);
+
+        // Faces of the row: interior law everywhere, then the edges.
+        T qw[N], qs[N];
+        row_faces(h, z, hN, zN, qxo, qxoN, qyo, qyoN, hL, zL, qyoL, qyoNL, qxoR, qxoNR, has_next,
+                  ph, qw, qs);
+        if (kEdge) {
+#pragma unroll
+          for (int k = 0; k < N; k++) {
+            const int c = cb + k;
+            if (c == 0) qw[k] = p.wf ? west_free(h[0], z[0], h[1], z[1], ph) : T(0);
+            else if (c >= nx) qw[k] = T(0);
+          }
+        }
+        if (!has_next) {
+#pragma unroll
+          for (int k = 0; k < N; k++) qs[k] = p.sf ? out_free(h[k], z[k], T(1), ph) : T(0);
+        }
+        const T qwR = __shfl_down_sync(0xffffffffu, qw[0], 1);
+        // East face of every cell.
+        T qe[N];
+#pragma unroll
+        for (int k = 0; k < N; k++) qe[k] = (k < N - 1) ? qw[k + 1] : qwR;
+        T qe_last = T(0);
+        if (kEdge) {
+#pragma unroll
+          for (int k = 0; k < N; k++) {
+            if (cb + k == nx - 1) {
+              qe[k] = p.ef ? out_free(h[k], z[k], T(1), ph) : T(0);
+              qe_last = qe[k];
             }
           }
         }
-        if (cb <= nx - 1 && nx - 1 < cb + N) Qxn[(long long)j * P + nx] = qe_last;
+        // Depth update of the owned cells.
+        T hn[N];
+#pragma unroll
+        for (int k = 0; k < N; k++) hn[k] = h[k];
+        const int sp_row = sp;
+        // Point sources (src/main.cpp:245-262), before rain and the update.
+        while (sp < sp_end && p.spec[sp].row == j) {
+          const SpecCell e = p.spec[sp];
+          if (own) {
+#pragma unroll
+            for (int k = 0; k < N; k++)
+              if (cb + k == e.col) hn[k] = apply_sources(hn[k], e, p, t, dt);
+          }
+          sp++;
+        }
+        update_cells(hn, qw, qe, qyn, qs, z, rain_on, rain_depth, dtT, dAT, dt_dA, ph.nodata);
+        // Point depth BCs (src/kernels.cpp:259-277), after the update.
+        for (int q = sp_row; q < sp; q++) {
+          const SpecCell e = p.spec[q];
+          if (own && e.bc >= 0) {
+            const T v = bc_depth<T>(e.bc, p, t);
+#pragma unroll
+            for (int k = 0; k < N; k++)
+              if (cb + k == e.col) hn[k] = v;
+          }
+        }
+        if (own) {
+          const long long r = (long long)j * P + cb;
+          const long long rs = r + P;
+          if (!kEdge || cb + N <= nx) {
+            st_vec(Hn + r, hn);
+            st_vec(Qxn + r, qw);
+            st_vec(Qyn + rs, qs);
+          } else {
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+              if (cb + k < nx) {
+                Hn[r + k] = hn[k];
+                Qxn[r + k] = qw[k];
+                Qyn[rs + k] = qs[k];
+              }
+            }
+          }
+          if (kEdge && cb <= nx - 1 && nx - 1 < cb + N) Qxn[(long long)j * P + nx] = qe_last;
+#pragma unroll
+          for (int k = 0; k < N; k++) {
+            if (!kEdge || cb + k < nx) {
+              const double hv = (double)hn[k];
+              if (z[k] != ph.nodata && hv > m_loc) m_loc = hv;
+              if (mass) {
+                v_loc += hv * p.dA;
+                if (hv > 0.01) a_loc += p.dA;
+              }
+            }
+          }
+        }
+        // Advance one row.
 #pragma unroll
         for (int k = 0; k < N; k++) {
-          if (cb + k < nx) {
-            const double hv = (double)hn[k];
-            if (z[k] != ph.nodata && hv > m_loc) m_loc = hv;
-            if (mass) {
-              v_loc += hv * p.dA;
-              if (hv > 0.01) a_loc += p.dA;
-            }
-          }
+          h[k] = hN[k];
+          z[k] = zN[k];
+          qxo[k] = qxoN[k];
+          qyo[k] = qyoN[k];
+          qyn[k] = qs[k];
         }
       }
-      // Advance one row.
-#pragma unroll
-      for (int k = 0; k < N; k++) {
-        h[k] = hN[k];
-        z[k] = zN[k];
-        qxo[k] = qxoN[k];
-        qyo[k] = qyoN[k];
-        qyn[k] = qs[k];
-      }
+    };
+    if (!failed) {
+#if AF_EDGE_SPLIT
+      const bool interior = (x0 > 0) && (x0 + OWN < nx);
+      if (interior) rows(BoolC<false>());
+      else rows(BoolC<true>());
+#else
+      rows(BoolC<true>());
+#endif
     }
+    if (failed) {
+      // Drain the copies still in flight into this warp's stages (bounded),
+      // then flag the control block so the loop stops with an error.
+      const int issued = min(nload, kc + kStages);
+      for (int k = kc; k < issued; k++)
+        mbar_wait_warp(&bar[(kglob + k) % kStages], (uint32_t)(((kglob + k) / kStages) & 1));
+      if (lane == 0) atomicExch(&ctl->status, 2);
+    }
+    kglob += nload;
   }
 
   // ----- block reductions: Hmax, and volume/area at mass-report steps -----
-  __shared__ double s_m[WX], s_v[WX], s_a[WX];
+  __shared__ double s_m[WY], s_v[WY], s_a[WY];
   __shared__ bool s_last;
   m_loc = warp_maxd(m_loc);
   if (mass) {
@@ -503,7 +828,7 @@ __global__ void __launch_bounds__(32 * WX) k_step(const StepParams p) {
   const unsigned bid = blockIdx.y * gridDim.x + blockIdx.x;
   if (threadIdx.x == 0) {
     double m = s_m[0], v = s_v[0], a = s_a[0];
-    for (int w = 1; w < WX; w++) {
+    for (int w = 1; w < WY; w++) {
       if (s_m[w] > m) m = s_m[w];
       v += s_v[w];
       a += s_a[w];
@@ -523,7 +848,7 @@ __global__ void __launch_bounds__(32 * WX) k_step(const StepParams p) {
 
   // ----- last block: fold the step into the control block -----
   __threadfence();
-  __shared__ double r_v[32 * WX], r_c[32 * WX], r_a[32 * WX];
+  __shared__ double r_v[32 * WY], r_c[32 * WY], r_a[32 * WY];
   if (mass) {
     double s = 0.0, c = 0.0, a = 0.0;
     for (unsigned b = threadIdx.x; b < nblocks; b += blockDim.x) {
@@ -571,7 +896,8 @@ __global__ void __launch_bounds__(32 * WX) k_step(const StepParams p) {
                                   : 0.0;
     // A non-positive or non-finite dt (a diverged state) would stall time:
     // stop the loop and report it instead.
-    const bool bad = !(dt > 0.0) || !(t_new < 1.0e300) || !(hmax == hmax);
+    const bool bad = !(dt > 0.0) || !(t_new < 1.0e300) || !(hmax == hmax) ||
+                     *(volatile int*)&ctl->status != 0;
     if (bad) ctl->status = 1;
     const int done = bad || !(t_new < ctl->t_stop) || step_new >= ctl->step_stop;
     ctl->done = done;
@@ -583,7 +909,13 @@ __global__ void __launch_bounds__(32 * WX) k_step(const StepParams p) {
 
 // Kernel entry points of the two precisions (defined in af_step_f64.cu and
 // af_step_f32.cu, which are compiled with different floating-point flags).
-const void* step_kernel_f64(int wx);
-const void* step_kernel_f32(int wx);
+// Launch variants: (warps per block, minimum resident blocks per SM).
+struct StepVariant {
+  int wy, minb;
+};
+constexpr int kStepVariants = 5;
+constexpr StepVariant kStepVariant[kStepVariants] = {{1, 16}, {1, 12}, {1, 20}, {4, 4}, {2, 8}};
+const void* step_kernel_f64(int variant);
+const void* step_kernel_f32(int variant);
 
 }  // namespace af

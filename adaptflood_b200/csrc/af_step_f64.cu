@@ -3,11 +3,14 @@
 #include "af_step.cuh"
 
 namespace af {
-const void* step_kernel_f64(int wx) {
-  switch (wx) {
-    case 1: return (const void*)&k_step<double, 1>;
-    case 2: return (const void*)&k_step<double, 2>;
-    default: return (const void*)&k_step<double, 4>;
+// Indices follow kStepVariant in af_step.cuh.
+const void* step_kernel_f64(int variant) {
+  switch (variant) {
+    case 1: return (const void*)&k_step<double, 1, 12>;
+    case 2: return (const void*)&k_step<double, 1, 20>;
+    case 3: return (const void*)&k_step<double, 4, 4>;
+    case 4: return (const void*)&k_step<double, 2, 8>;
+    default: return (const void*)&k_step<double, 1, 16>;
   }
 }
 }  // namespace af
