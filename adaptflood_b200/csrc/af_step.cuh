@@ -183,19 +183,19 @@ __device__ inline T face_flux(T z0, T h0, T z1, T h1, T q0, T qa, T qb, T qc, T 
 // FREE edges (src/kernels.cpp:154-248).  West also needs the cell east of
 // the edge cell.
 template <typename T>
-__device__ inline T west_free(T h0, T z0, T h1, T z1, const Phys<T>& ph) {
-  if (z0 == ph.nodata || h0 < T(0.001)) return T(0);
+__device__ inline T west_free(T h0, T z0, T h1, T z1, T g, T dx, T nodata) {
+  if (z0 == nodata || h0 < T(0.001)) return T(0);
   T y0 = z0 + h0, y1 = z1 + h1;
   if (y0 > z0) {
-    T Sf = (y1 - y0) / ph.dx;
-    if (Sf < 0) return -h0 * sqrt(ph.g * h0) * ph.dx * T(0.5);
+    T Sf = (y1 - y0) / dx;
+    if (Sf < 0) return -h0 * sqrt(g * h0) * dx * T(0.5);
   }
   return T(0);
 }
 template <typename T>
-__device__ inline T out_free(T h0, T z0, T sign, const Phys<T>& ph) {
-  if (z0 == ph.nodata || h0 < T(0.001)) return T(0);
-  if (h0 > T(0.001)) return sign * h0 * sqrt(ph.g * h0) * ph.dx * T(0.5);
+__device__ inline T out_free(T h0, T z0, T sign, T g, T dx, T nodata) {
+  if (z0 == nodata || h0 < T(0.001)) return T(0);
+  if (h0 > T(0.001)) return sign * h0 * sqrt(g * h0) * dx * T(0.5);
   return T(0);
 }
 
@@ -219,32 +219,46 @@ __device__ inline void kahan_add(double& s, double& c, double x) {
   s = t;
 }
 
+// Special-cell helpers (a handful of calls per step) take scalar arguments,
+// not the parameter block, so they never force it into local memory.
+struct SeriesTable {
+  const int* type;
+  const double* value;
+  const int* off;
+  const double* times;
+  const double* vals;
+  const unsigned char* sorted;
+};
+
+// src/main.cpp:246-259 for the sources [s0, s1) of one cell, in file order.
 template <typename T>
-__device__ inline T apply_sources(T h, const SpecCell& e, const StepParams& p, double t, double dt) {
-  for (int s = e.s0; s < e.s1; s++) {
+__device__ inline T apply_sources(T h, int s0, int s1, SeriesTable tb, double dx, double dA,
+                                        double t, double dt) {
+  for (int s = s0; s < s1; s++) {
     double v;
-    if (p.src_type[s] == AF_BC_QFIX) {
-      v = p.src_value[s];
+    if (tb.type[s] == AF_BC_QFIX) {
+      v = tb.value[s];
     } else {
-      int o = p.src_off[s];
-      v = interp_series(p.src_times + o, p.src_vals + o, p.src_off[s + 1] - o, p.src_value[s], t,
-                        p.src_sorted[s] != 0);
+      const int o = tb.off[s];
+      v = interp_series(tb.times + o, tb.vals + o, tb.off[s + 1] - o, tb.value[s], t,
+                        tb.sorted[s] != 0);
     }
-    double ps = v * p.dx * dt / p.dA;  // src/main.cpp:253
+    const double ps = v * dx * dt / dA;  // src/main.cpp:253
     h = h + T(ps);
     if (h < T(0)) h = T(0);
   }
   return h;
 }
 
+// src/kernels.cpp:266-273 (FREE -> 0, HFIX -> value, HVAR -> value at t).
 template <typename T>
-__device__ inline T bc_depth(int b, const StepParams& p, double t) {
-  int ty = p.bc_type[b];
+__device__ inline T bc_depth(int b, SeriesTable tb, double t) {
+  const int ty = tb.type[b];
   if (ty == 1) return T(0);
-  if (ty == 2) return T(p.bc_value[b]);
-  int o = p.bc_off[b];
-  return T(interp_series(p.bc_times + o, p.bc_vals + o, p.bc_off[b + 1] - o, p.bc_value[b], t,
-                         p.bc_sorted[b] != 0));
+  if (ty == 2) return T(tb.value[b]);
+  const int o = tb.off[b];
+  return T(interp_series(tb.times + o, tb.vals + o, tb.off[b + 1] - o, tb.value[b], t,
+                         tb.sorted[b] != 0));
 }
 
 // ------------------------------------------------------------ row faces
@@ -377,7 +391,10 @@ __device__ inline void row_faces(const float (&h)[4], const float (&z)[4], const
 // read their 16 bytes, and the stage is refilled kStages rows ahead.  Every
 // wait is bounded (kWaitLimit polls); on time-out the warp stops, drains its
 // copies in flight (bounded again) and flags the control block.
-constexpr int kStages = 4;
+#ifndef AF_STAGES
+#define AF_STAGES 3
+#endif
+constexpr int kStages = AF_STAGES;  // ring depth (rows in flight per warp, incl. the one in use)
 // Code-shape knobs of the fused step (compile time): unroll factor of the row
 // loop, and whether x-interior strips get their own copy of the row body
 // without per-column edge tests.
@@ -531,7 +548,12 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
   ph.dxinv = T(1.0 / p.dx);
   ph.gdt_fn2 = T(p.g * dt * p.fpn * p.fpn);
 
+  const SeriesTable src_tb{p.src_type, p.src_value, p.src_off, p.src_times, p.src_vals,
+                           p.src_sorted};
+  const SeriesTable bc_tb{p.bc_type, p.bc_value, p.bc_off, p.bc_times, p.bc_vals, p.bc_sorted};
   double m_loc = -DBL_MAX, v_loc = 0.0, a_loc = 0.0;
+  T m_cell = T(-FLT_MAX);  // running max of this lane's valid cells, state precision
+  bool any_cell = false;
   bool failed = false;
 
   const int nx = p.nx, ny = p.ny, P = p.P;
@@ -632,7 +654,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
       // North faces of row j0.
       if (j0 == 0) {
 #pragma unroll
-        for (int k = 0; k < N; k++) qyn[k] = p.nf ? out_free(h[k], z[k], T(-1), ph) : T(0);
+        for (int k = 0; k < N; k++) qyn[k] = p.nf ? out_free(h[k], z[k], T(-1), ph.g, ph.dx, ph.nodata) : T(0);
         if (own) {
           if (cb + N <= nx) {
             st_vec(Qyn + cb, qyn);
@@ -700,13 +722,13 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
 #pragma unroll
           for (int k = 0; k < N; k++) {
             const int c = cb + k;
-            if (c == 0) qw[k] = p.wf ? west_free(h[0], z[0], h[1], z[1], ph) : T(0);
+            if (c == 0) qw[k] = p.wf ? west_free(h[0], z[0], h[1], z[1], ph.g, ph.dx, ph.nodata) : T(0);
             else if (c >= nx) qw[k] = T(0);
           }
         }
         if (!has_next) {
 #pragma unroll
-          for (int k = 0; k < N; k++) qs[k] = p.sf ? out_free(h[k], z[k], T(1), ph) : T(0);
+          for (int k = 0; k < N; k++) qs[k] = p.sf ? out_free(h[k], z[k], T(1), ph.g, ph.dx, ph.nodata) : T(0);
         }
         const T qwR = __shfl_down_sync(0xffffffffu, qw[0], 1);
         // East face of every cell.
@@ -718,7 +740,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
 #pragma unroll
           for (int k = 0; k < N; k++) {
             if (cb + k == nx - 1) {
-              qe[k] = p.ef ? out_free(h[k], z[k], T(1), ph) : T(0);
+              qe[k] = p.ef ? out_free(h[k], z[k], T(1), ph.g, ph.dx, ph.nodata) : T(0);
               qe_last = qe[k];
             }
           }
@@ -734,7 +756,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
           if (own) {
 #pragma unroll
             for (int k = 0; k < N; k++)
-              if (cb + k == e.col) hn[k] = apply_sources(hn[k], e, p, t, dt);
+              if (cb + k == e.col) hn[k] = apply_sources(hn[k], e.s0, e.s1, src_tb, p.dx, p.dA, t, dt);
           }
           sp++;
         }
@@ -743,7 +765,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
         for (int q = sp_row; q < sp; q++) {
           const SpecCell e = p.spec[q];
           if (own && e.bc >= 0) {
-            const T v = bc_depth<T>(e.bc, p, t);
+            const T v = bc_depth<T>(e.bc, bc_tb, t);
 #pragma unroll
             for (int k = 0; k < N; k++)
               if (cb + k == e.col) hn[k] = v;
@@ -770,9 +792,12 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
 #pragma unroll
           for (int k = 0; k < N; k++) {
             if (!kEdge || cb + k < nx) {
-              const double hv = (double)hn[k];
-              if (z[k] != ph.nodata && hv > m_loc) m_loc = hv;
+              if (z[k] != ph.nodata) {
+                any_cell = true;
+                if (hn[k] > m_cell) m_cell = hn[k];
+              }
               if (mass) {
+                const double hv = (double)hn[k];
                 v_loc += hv * p.dA;
                 if (hv > 0.01) a_loc += p.dA;
               }
@@ -809,6 +834,10 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
     }
     kglob += nload;
   }
+
+  // A valid cell's depth is finite (NaN never wins a comparison), and in
+  // FP64 m_cell is exact; a lane with no valid cell keeps the identity.
+  if (any_cell && (double)m_cell > m_loc) m_loc = (double)m_cell;
 
   // ----- block reductions: Hmax, and volume/area at mass-report steps -----
   __shared__ double s_m[WY], s_v[WY], s_a[WY];
