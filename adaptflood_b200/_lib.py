@@ -54,7 +54,7 @@ class ForcingDesc(C.Structure):
 _lock = threading.Lock()
 _lib = None
 
-_vp, _i, _d, _i64 = C.c_void_p, C.c_int, C.c_double, C.c_int64
+_vp, _i, _d, _i64, _u64 = C.c_void_p, C.c_int, C.c_double, C.c_int64, C.c_uint64
 _SIGS = {
     "af_strerror": (C.c_char_p, [_i]),
     "af_last_cuda_error": (C.c_char_p, []),
@@ -83,6 +83,29 @@ _SIGS = {
     "af_sim_velocity": (_i, [_vp, _vp, _vp]),
     "af_sim_volume": (_i, [_vp, _vp, _vp]),
     "af_sim_mass_series": (_i, [_vp, _vp, _vp, _vp, _i, _vp]),
+    "af_batch_create": (_i, [_i, _i, _u64, _i, _vp]),
+    "af_batch_destroy": (_i, [_vp]),
+    "af_batch_size_class": (_i, [_i, _i]),
+    "af_batch_set_rows": (_i, [_vp, _i, _i]),
+    "af_batch_get_rows": (_i, [_vp, _i]),
+    "af_batch_footprint": (_i, [_vp, _vp, _vp, _d, _vp]),
+    "af_batch_add": (_i, [_vp, _vp, _vp, _vp, _vp, _d, _vp]),
+    "af_batch_remove": (_i, [_vp, _i]),
+    "af_batch_launch": (_i, [_vp, _i64, _i]),
+    "af_batch_attention": (_i, [_vp]),
+    "af_batch_query": (_i, [_vp]),
+    "af_batch_sync": (_i, [_vp]),
+    "af_batch_run": (_i, [_vp, _i64, _vp]),
+    "af_batch_slot_status": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    "af_batch_get_state": (_i, [_vp, _i, _vp, _vp, _vp]),
+    "af_batch_mass_series": (_i, [_vp, _i, _vp, _vp, _vp, _i, _vp]),
+    "af_batch_info": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "af_batch_stream": (_vp, [_vp]),
+    "af_arena_create": (_i, [_u64, _vp]),
+    "af_arena_destroy": (_i, [_vp]),
+    "af_arena_alloc": (_i, [_vp, _u64, _vp]),
+    "af_arena_free": (_i, [_vp, _u64]),
+    "af_arena_stats": (_i, [_vp, _vp, _vp, _vp]),
     "af_scenario_load": (_i, [C.c_char_p, _vp]),
     "af_scenario_free": (None, [_vp]),
     "af_scenario_get": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),

@@ -35,9 +35,10 @@ UNITS = [
     ("af_step_f64.cu", EXACT),
     ("af_step_f32.cu", FAST),
     ("af_sim.cu", EXACT),
+    ("af_batch.cu", EXACT),
 ]
-HOST_UNITS = ["af_io.cpp"]
-HEADERS = ["af_common.cuh", "af_step.cuh"]
+HOST_UNITS = ["af_io.cpp", "af_arena.cpp"]
+HEADERS = ["af_common.cuh", "af_step.cuh", "af_simcore.cuh", "af_arena.h"]
 
 
 def _newer(target: str, deps) -> bool:

@@ -1,14 +1,6 @@
 // af_sim.cu -- the simulation layer: device-resident state, forcing tables,
-// special-cell lists, and the CUDA graph that runs the time loop.
-//
-// Memory layout in HBM (per precision T, N = 16 bytes / sizeof(T)):
-//   every array has a front guard of kGuard elements and rows of pitch P,
-//   P >= nsx*OWN + N rounded up to 32 elements, so every 16-byte lane vector
-//   of every strip (halo lanes included) is inside the allocation and aligned;
-//   H[2], DEM: ny rows of cells (column i = cell i)
-//   Qx[2]:     ny rows of x-faces (column i = west face of cell i, i <= nx)
-//   Qy[2]:     ny+1 rows of y-faces (row j = north face of row j)
-// Padding is zero and never read into an owned result.
+// special-cell lists, and the CUDA graph that runs the time loop of one grid.
+// The padded field layout is described in af_simcore.cuh.
 //
 // The time loop (src/main.cpp:227 `while (t < sim_time)`) is one graph
 // launch: a begin kernel sets the stop condition, then a conditional WHILE
@@ -21,11 +13,10 @@
 #include <numeric>
 #include <vector>
 
-#include "af_step.cuh"
+#include "af_simcore.cuh"
 
 namespace af {
 
-constexpr int kGuard = 64;
 constexpr int kMassCap = 1 << 16;
 
 struct DevBuf {
@@ -48,34 +39,124 @@ static int upload(DevBuf& b, const std::vector<V>& v, cudaStream_t st) {
   return AF_OK;
 }
 
-static bool non_decreasing(const double* t, int n) {
-  for (int i = 0; i + 1 < n; i++)
-    if (!(t[i] <= t[i + 1])) return false;
-  for (int i = 0; i < n; i++)
-    if (t[i] != t[i]) return false;
-  return true;
+int check_case(const af_case_desc* c, const af_forcing_desc* f) {
+  if (!c || !f) return AF_EINVAL;
+  if (c->nx < 2 || c->ny < 2) return AF_EINVAL;
+  if (!(c->dx > 0.0) || c->theta != 1.0) return AF_EINVAL;
+  if ((long long)(c->nx + 1) * (c->ny + 1) > 0x7FFFFFFFLL) return AF_ERANGE;
+  if (f->n_flow < 0 || f->n_other < 0 || f->n_rain < 0) return AF_EINVAL;
+  const long long ncell = (long long)c->nx * c->ny;
+  for (int k = 0; k < f->n_flow; k++)
+    if (f->flow_idx[k] < 0 || f->flow_idx[k] >= ncell) return AF_ERANGE;
+  for (int k = 0; k < f->n_other; k++)
+    if (f->other_idx[k] < 0 || f->other_idx[k] >= ncell) return AF_ERANGE;
+  return AF_OK;
 }
 
-// ------------------------------------------------------------- kernels
-template <typename T>
-__global__ void k_hmax_int(const T* __restrict__ H, const T* __restrict__ Z, int nx, int ny,
-                           int P, double nodata, unsigned long long* acc) {
-  double m = -DBL_MAX;
-  const T nd = T(nodata);
-  long long n = (long long)nx * ny;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-       k += (long long)gridDim.x * blockDim.x) {
-    long long j = k / nx, i = k - j * nx;
-    double h = (double)H[j * P + i];
-    if (Z[j * P + i] != nd && h > m) m = h;
+void build_tables(const af_case_desc* c, const af_forcing_desc* f, int own, int R, int nsx,
+                  int nsy, HostTables& t) {
+  const int nx = c->nx;
+  // ---- point sources, stably sorted by cell (file order kept per cell)
+  std::vector<int> order(f->n_flow);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return f->flow_idx[a] < f->flow_idx[b]; });
+  t.src_off.assign(1, 0);
+  for (int k : order) {
+    t.src_type.push_back(f->flow_type[k]);
+    t.src_value.push_back(f->flow_value[k]);
+    int n = 0;
+    if (f->flow_type[k] == AF_BC_QVAR) {
+      int o = f->flow_off[k];
+      n = f->flow_off[k + 1] - o;
+      t.src_times.insert(t.src_times.end(), f->flow_times + o, f->flow_times + o + n);
+      t.src_vals.insert(t.src_vals.end(), f->flow_vals + o, f->flow_vals + o + n);
+      t.src_sorted.push_back(non_decreasing(f->flow_times + o, n) ? 1 : 0);
+    } else {
+      t.src_sorted.push_back(1);
+    }
+    t.src_off.push_back(t.src_off.back() + n);
   }
-  m = warp_maxd(m);
-  if ((threadIdx.x & 31) == 0 && m > -DBL_MAX) atomicMax(acc, ord_encode(m));
-}
-
-__global__ void k_ctl_fold_hmax(SimCtl* ctl) {
-  ctl->hmax = ord_decode(ctl->hmax_acc);
-  ctl->hmax_acc = ord_encode(-DBL_MAX);
+  // ---- point depth BCs: the last effective one per cell wins (file order)
+  t.bc_type.resize(f->n_other);
+  t.bc_off.assign(f->n_other + 1, 0);
+  t.bc_value.resize(f->n_other);
+  t.bc_sorted.resize(f->n_other);
+  for (int k = 0; k < f->n_other; k++) {
+    t.bc_type[k] = f->other_type[k];
+    t.bc_value[k] = f->other_value[k];
+    int n = 0;
+    if (t.bc_type[k] == AF_BC_HVAR) {
+      int o = f->other_off[k];
+      n = f->other_off[k + 1] - o;
+      t.bc_times.insert(t.bc_times.end(), f->other_times + o, f->other_times + o + n);
+      t.bc_vals.insert(t.bc_vals.end(), f->other_vals + o, f->other_vals + o + n);
+    }
+    t.bc_off[k + 1] = t.bc_off[k] + n;
+    t.bc_sorted[k] = non_decreasing(t.bc_times.data() + t.bc_off[k], n) ? 1 : 0;
+  }
+  // ---- special cells
+  struct Ent {
+    long long key;
+    SpecCell e;
+  };
+  std::vector<Ent> ents;
+  {
+    size_t k = 0;
+    std::vector<std::pair<int, int>> last_bc;  // (cell, bc)
+    for (int b = 0; b < f->n_other; b++)
+      if (t.bc_type[b] == 1 || t.bc_type[b] == 2 || t.bc_type[b] == 3)
+        last_bc.push_back({f->other_idx[b], b});
+    std::stable_sort(last_bc.begin(), last_bc.end(),
+                     [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+                       return a.first < b.first;
+                     });
+    std::vector<std::pair<int, int>> bc_of;  // cell -> last bc
+    for (size_t q = 0; q < last_bc.size(); q++)
+      if (q + 1 == last_bc.size() || last_bc[q + 1].first != last_bc[q].first)
+        bc_of.push_back(last_bc[q]);
+    size_t qb = 0;
+    auto emit = [&](int cell, int s0, int s1, int bc) {
+      SpecCell e{};
+      e.row = cell / nx;
+      e.col = cell % nx;
+      e.s0 = s0;
+      e.s1 = s1;
+      e.bc = bc;
+      int sx = e.col / own, sy = e.row / R;
+      long long strip = (long long)sy * nsx + sx;
+      ents.push_back({(strip << 40) | ((long long)e.row << 20) | 0, e});
+    };
+    // merge the sorted source cells with the sorted bc cells
+    while (k < order.size() || qb < bc_of.size()) {
+      int cs = k < order.size() ? f->flow_idx[order[k]] : 0x7FFFFFFF;
+      int cbc = qb < bc_of.size() ? bc_of[qb].first : 0x7FFFFFFF;
+      int cell = std::min(cs, cbc);
+      int s0 = (int)k;
+      while (k < order.size() && f->flow_idx[order[k]] == cell) k++;
+      int bc = -1;
+      if (cbc == cell) {
+        bc = bc_of[qb].second;
+        qb++;
+      }
+      emit(cell, s0, (int)k, bc);
+    }
+  }
+  std::stable_sort(ents.begin(), ents.end(), [](const Ent& a, const Ent& b) {
+    if (a.key != b.key) return a.key < b.key;
+    return a.e.col < b.e.col;
+  });
+  const long long nstrips = (long long)nsx * nsy;
+  t.spec_off.assign(nstrips + 1, 0);
+  t.spec.clear();
+  for (auto& e : ents) {
+    t.spec_off[(e.key >> 40) + 1]++;
+    t.spec.push_back(e.e);
+  }
+  for (long long q = 0; q < nstrips; q++) t.spec_off[q + 1] += t.spec_off[q];
+  t.rain_times.assign(f->rain_times, f->rain_times + f->n_rain);
+  t.rain_rates.assign(f->rain_rates, f->rain_rates + f->n_rain);
+  t.rain_sorted = non_decreasing(t.rain_times.data(), f->n_rain) ? 1 : 0;
 }
 
 // Sets the stop condition of one launch: the loop runs while t < t_stop and
@@ -90,68 +171,6 @@ __global__ void k_begin(SimCtl* ctl, double t_stop, long long max_steps,
   ctl->done = done;
   ctl->arrive = 0u;
   if (use_cond) cudaGraphSetConditional(cond, done ? 0u : 1u);
-}
-
-// ComputeVelocity_GPU (src/kernels.cpp:293-351) on the padded layout.
-template <typename T>
-__global__ void k_velocity_int(const T* __restrict__ H, const T* __restrict__ Z,
-                               const T* __restrict__ Qx, const T* __restrict__ Qy, int nx,
-                               int j0, int j1, int P, double dx, double nodata,
-                               double* __restrict__ Vx, double* __restrict__ Vy) {
-  long long n = (long long)nx * (j1 - j0);
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-       k += (long long)gridDim.x * blockDim.x) {
-    int jr = (int)(k / nx), i = (int)(k - (long long)jr * nx);
-    long long r = (long long)(j0 + jr) * P;
-    double z = (double)Z[r + i], h = (double)H[r + i];
-    if (z == (double)T(nodata) || h < 0.001) {
-      Vx[k] = 0.0;
-      Vy[k] = 0.0;
-      continue;
-    }
-    double hflow = h;
-    if (hflow < 0.001) hflow = 0.001;
-    double ql = (double)Qx[r + i], qr = (double)Qx[r + i + 1];
-    double vl = (fabs(ql) > 1e-10) ? ql / dx / hflow : 0.0;
-    double vr = (fabs(qr) > 1e-10) ? qr / dx / hflow : 0.0;
-    Vx[k] = (fabs(vl) > fabs(vr)) ? vl : vr;
-    double qt = (double)Qy[r + i], qb = (double)Qy[r + P + i];
-    double vt = (fabs(qt) > 1e-10) ? qt / dx / hflow : 0.0;
-    double vb = (fabs(qb) > 1e-10) ? qb / dx / hflow : 0.0;
-    Vy[k] = (fabs(vt) > fabs(vb)) ? vt : vb;
-  }
-}
-
-// Volume and flooded area of the state (src/main.cpp:293-298), fixed order.
-template <typename T>
-__global__ void k_volume_int(const T* __restrict__ H, int nx, int ny, int P, double dA,
-                             double* __restrict__ part) {
-  long long n = (long long)nx * ny;
-  long long chunk = (n + gridDim.x - 1) / gridDim.x;
-  long long lo = blockIdx.x * chunk, hi = min(lo + chunk, n);
-  double s = 0.0, c = 0.0, a = 0.0;
-  for (long long k = lo + threadIdx.x; k < hi; k += blockDim.x) {
-    long long j = k / nx, i = k - j * nx;
-    double h = (double)H[j * P + i];
-    kahan_add(s, c, h * dA);
-    if (h > 0.01) a += dA;
-  }
-  __shared__ double ss[256], sc[256], sa[256];
-  ss[threadIdx.x] = s;
-  sc[threadIdx.x] = c;
-  sa[threadIdx.x] = a;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double S = 0.0, C = 0.0, A = 0.0;
-    for (int k = 0; k < (int)blockDim.x; k++) {
-      kahan_add(S, C, ss[k]);
-      C += sc[k];
-      A += sa[k];
-    }
-    part[3 * blockIdx.x] = S;
-    part[3 * blockIdx.x + 1] = C;
-    part[3 * blockIdx.x + 2] = A;
-  }
 }
 
 // ----------------------------------------------------------- the object
@@ -298,13 +317,6 @@ static int write_ctl(Sim& s) {
   return AF_OK;
 }
 
-static double first_mass_after(double t, double mass_int) {
-  if (!(mass_int > 0.0)) return 0.0;
-  double nm = mass_int;  // src/main.cpp:200, advanced as :303 does
-  while (nm <= t) nm += mass_int;
-  return nm;
-}
-
 static int build_graph(Sim& s) {
   // AF_SIM_DIRECT_LAUNCH=1 launches the same step kernel from the host in
   // batches instead of through the conditional graph: profilers cannot see
@@ -358,15 +370,7 @@ static int create(const af_case_desc* c, const af_forcing_desc* f, const double*
                   const double* h0, int precision, int device, Sim** out) {
   if (!c || !f || !dem || !out) return AF_EINVAL;
   if (precision != AF_PREC_F64 && precision != AF_PREC_F32) return AF_EINVAL;
-  if (c->nx < 2 || c->ny < 2) return AF_EINVAL;
-  if (!(c->dx > 0.0) || c->theta != 1.0) return AF_EINVAL;
-  if ((long long)(c->nx + 1) * (c->ny + 1) > 0x7FFFFFFFLL) return AF_ERANGE;
-  if (f->n_flow < 0 || f->n_other < 0 || f->n_rain < 0) return AF_EINVAL;
-  const long long ncell = (long long)c->nx * c->ny;
-  for (int k = 0; k < f->n_flow; k++)
-    if (f->flow_idx[k] < 0 || f->flow_idx[k] >= ncell) return AF_ERANGE;
-  for (int k = 0; k < f->n_other; k++)
-    if (f->other_idx[k] < 0 || f->other_idx[k] >= ncell) return AF_ERANGE;
+  AF_TRY(check_case(c, f));
 
   std::unique_ptr<Sim> s(new Sim());
   s->device = device;
@@ -379,12 +383,11 @@ static int create(const af_case_desc* c, const af_forcing_desc* f, const double*
   AF_CUDA(cudaMallocHost(&s->pinned_ctl, sizeof(SimCtl)));
   pick_shape(*s);
   const int own = 30 * s->N;
-  int P = s->nsx * own + s->N;
-  P = (P + 31) / 32 * 32;
+  const int P = row_pitch(c->nx, s->N);
   s->P = P;
   const int nx = c->nx, ny = c->ny;
-  s->cells_elems = (size_t)kGuard * 2 + (size_t)ny * P;
-  s->qy_elems = (size_t)kGuard * 2 + (size_t)(ny + 1) * P;
+  s->cells_elems = cell_elems(ny, P);
+  s->qy_elems = qy_elems(ny, P);
   for (int b = 0; b < 2; b++) {
     AF_TRY(alloc_field(s->H[b], s->cells_elems, s->esize));
     AF_TRY(alloc_field(s->Qx[b], s->cells_elems, s->esize));
@@ -398,124 +401,27 @@ static int create(const af_case_desc* c, const af_forcing_desc* f, const double*
   AF_TRY(put_field(*s, s->DEM, dem, ny, nx, nx));
   if (h0) AF_TRY(put_field(*s, s->H[0], h0, ny, nx, nx));
 
-  // ---- point sources, stably sorted by cell (file order kept per cell)
-  std::vector<int> order(f->n_flow);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int a, int b) { return f->flow_idx[a] < f->flow_idx[b]; });
-  std::vector<int> st_type, st_off(1, 0);
-  std::vector<double> st_value, st_times, st_vals;
-  std::vector<unsigned char> st_sorted;
-  for (int k : order) {
-    st_type.push_back(f->flow_type[k]);
-    st_value.push_back(f->flow_value[k]);
-    int n = 0;
-    if (f->flow_type[k] == AF_BC_QVAR) {
-      int o = f->flow_off[k];
-      n = f->flow_off[k + 1] - o;
-      st_times.insert(st_times.end(), f->flow_times + o, f->flow_times + o + n);
-      st_vals.insert(st_vals.end(), f->flow_vals + o, f->flow_vals + o + n);
-      st_sorted.push_back(non_decreasing(f->flow_times + o, n) ? 1 : 0);
-    } else {
-      st_sorted.push_back(1);
-    }
-    st_off.push_back(st_off.back() + n);
-  }
-  // ---- point depth BCs: the last effective one per cell wins (file order)
-  std::vector<int> bt(f->n_other), bo(f->n_other + 1, 0);
-  std::vector<double> bv(f->n_other), btimes, bvals;
-  std::vector<unsigned char> bsorted(f->n_other);
-  for (int k = 0; k < f->n_other; k++) {
-    bt[k] = f->other_type[k];
-    bv[k] = f->other_value[k];
-    int n = 0;
-    if (bt[k] == AF_BC_HVAR) {
-      int o = f->other_off[k];
-      n = f->other_off[k + 1] - o;
-      btimes.insert(btimes.end(), f->other_times + o, f->other_times + o + n);
-      bvals.insert(bvals.end(), f->other_vals + o, f->other_vals + o + n);
-    }
-    bo[k + 1] = bo[k] + n;
-    bsorted[k] = non_decreasing(btimes.data() + bo[k], n) ? 1 : 0;
-  }
-  // ---- special cells
-  struct Ent {
-    long long key;
-    SpecCell e;
-  };
-  std::vector<Ent> ents;
-  {
-    size_t k = 0;
-    std::vector<std::pair<int, int>> last_bc;  // (cell, bc)
-    for (int b = 0; b < f->n_other; b++)
-      if (bt[b] == 1 || bt[b] == 2 || bt[b] == 3) last_bc.push_back({f->other_idx[b], b});
-    std::stable_sort(last_bc.begin(), last_bc.end(),
-                     [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
-                       return a.first < b.first;
-                     });
-    std::vector<std::pair<int, int>> bc_of;  // cell -> last bc
-    for (size_t q = 0; q < last_bc.size(); q++)
-      if (q + 1 == last_bc.size() || last_bc[q + 1].first != last_bc[q].first)
-        bc_of.push_back(last_bc[q]);
-    size_t qb = 0;
-    auto emit = [&](int cell, int s0, int s1, int bc) {
-      SpecCell e{};
-      e.row = cell / nx;
-      e.col = cell % nx;
-      e.s0 = s0;
-      e.s1 = s1;
-      e.bc = bc;
-      int sx = e.col / own, sy = e.row / s->R;
-      long long strip = (long long)sy * s->nsx + sx;
-      ents.push_back({(strip << 40) | ((long long)e.row << 20) | 0, e});
-    };
-    // merge the sorted source cells with the sorted bc cells
-    while (k < order.size() || qb < bc_of.size()) {
-      int cs = k < order.size() ? f->flow_idx[order[k]] : 0x7FFFFFFF;
-      int cbc = qb < bc_of.size() ? bc_of[qb].first : 0x7FFFFFFF;
-      int cell = std::min(cs, cbc);
-      int s0 = (int)k;
-      while (k < order.size() && f->flow_idx[order[k]] == cell) k++;
-      int bc = -1;
-      if (cbc == cell) {
-        bc = bc_of[qb].second;
-        qb++;
-      }
-      emit(cell, s0, (int)k, bc);
-    }
-  }
-  std::stable_sort(ents.begin(), ents.end(), [](const Ent& a, const Ent& b) {
-    if (a.key != b.key) return a.key < b.key;
-    return a.e.col < b.e.col;
-  });
-  const long long nstrips = (long long)s->nsx * s->nsy;
-  std::vector<int> soff(nstrips + 1, 0);
-  std::vector<SpecCell> spec;
-  for (auto& e : ents) {
-    soff[(e.key >> 40) + 1]++;
-    spec.push_back(e.e);
-  }
-  for (long long q = 0; q < nstrips; q++) soff[q + 1] += soff[q];
-
-  AF_TRY(upload(s->src_type, st_type, s->st));
-  AF_TRY(upload(s->src_value, st_value, s->st));
-  AF_TRY(upload(s->src_off, st_off, s->st));
-  AF_TRY(upload(s->src_times, st_times, s->st));
-  AF_TRY(upload(s->src_vals, st_vals, s->st));
-  AF_TRY(upload(s->src_sorted, st_sorted, s->st));
-  AF_TRY(upload(s->bc_type, bt, s->st));
-  AF_TRY(upload(s->bc_value, bv, s->st));
-  AF_TRY(upload(s->bc_off, bo, s->st));
-  AF_TRY(upload(s->bc_times, btimes, s->st));
-  AF_TRY(upload(s->bc_vals, bvals, s->st));
-  AF_TRY(upload(s->bc_sorted, bsorted, s->st));
-  s->rain_t.assign(f->rain_times, f->rain_times + f->n_rain);
-  s->rain_r.assign(f->rain_rates, f->rain_rates + f->n_rain);
+  HostTables tb;
+  build_tables(c, f, own, s->R, s->nsx, s->nsy, tb);
+  AF_TRY(upload(s->src_type, tb.src_type, s->st));
+  AF_TRY(upload(s->src_value, tb.src_value, s->st));
+  AF_TRY(upload(s->src_off, tb.src_off, s->st));
+  AF_TRY(upload(s->src_times, tb.src_times, s->st));
+  AF_TRY(upload(s->src_vals, tb.src_vals, s->st));
+  AF_TRY(upload(s->src_sorted, tb.src_sorted, s->st));
+  AF_TRY(upload(s->bc_type, tb.bc_type, s->st));
+  AF_TRY(upload(s->bc_value, tb.bc_value, s->st));
+  AF_TRY(upload(s->bc_off, tb.bc_off, s->st));
+  AF_TRY(upload(s->bc_times, tb.bc_times, s->st));
+  AF_TRY(upload(s->bc_vals, tb.bc_vals, s->st));
+  AF_TRY(upload(s->bc_sorted, tb.bc_sorted, s->st));
+  s->rain_t = tb.rain_times;
+  s->rain_r = tb.rain_rates;
   s->n_rain = f->n_rain;
   AF_TRY(upload(s->rain_times, s->rain_t, s->st));
   AF_TRY(upload(s->rain_rates, s->rain_r, s->st));
-  AF_TRY(upload(s->spec_off, soff, s->st));
-  AF_TRY(upload(s->spec, spec, s->st));
+  AF_TRY(upload(s->spec_off, tb.spec_off, s->st));
+  AF_TRY(upload(s->spec, tb.spec, s->st));
   const size_t nblocks = (size_t)s->grid.x * s->grid.y;
   AF_TRY(alloc_field(s->partials, nblocks * 3 + 3, 8));
   AF_TRY(alloc_field(s->mass_series, (size_t)kMassCap * 3, 8));
@@ -578,7 +484,7 @@ static int create(const af_case_desc* c, const af_forcing_desc* f, const double*
   p.rain_times = (const double*)s->rain_times.p;
   p.rain_rates = (const double*)s->rain_rates.p;
   p.n_rain = s->n_rain;
-  p.rain_sorted = non_decreasing(s->rain_t.data(), s->n_rain) ? 1 : 0;
+  p.rain_sorted = tb.rain_sorted;
   p.spec_off = (const int*)s->spec_off.p;
   p.spec = (const SpecCell*)s->spec.p;
   p.ctl = static_cast<SimCtl*>(s->ctl.p);

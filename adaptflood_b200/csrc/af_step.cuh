@@ -49,7 +49,7 @@ struct SimCtl {
   long long step;     // steps taken so far
   long long step_stop;  // ... and step < step_stop
   unsigned long long hmax_acc;  // ordered-bits accumulator of this step's Hmax
-  unsigned int arrive;          // blocks finished in this step
+  unsigned int arrive;          // blocks (one grid) or strips (batch) finished in this step
   int done;
   int parity;         // buffer holding the current state
   int mass_count;     // entries recorded in the mass series
@@ -120,18 +120,6 @@ __device__ inline T gmaxT(T a, T b) { return (a > b) ? a : b; }  // src/types.hp
 template <typename T>
 __device__ inline T gminT(T a, T b) { return (a < b) ? a : b; }  // src/types.hpp:15
 
-__device__ inline void ld_vec(const double* p, double (&v)[2]) {
-  double2 t = __ldg(reinterpret_cast<const double2*>(p));
-  v[0] = t.x;
-  v[1] = t.y;
-}
-__device__ inline void ld_vec(const float* p, float (&v)[4]) {
-  float4 t = __ldg(reinterpret_cast<const float4*>(p));
-  v[0] = t.x;
-  v[1] = t.y;
-  v[2] = t.z;
-  v[3] = t.w;
-}
 __device__ inline void st_vec(double* p, const double (&v)[2]) {
   *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
 }
@@ -139,46 +127,12 @@ __device__ inline void st_vec(float* p, const float (&v)[4]) {
   *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
-// pow(hflow, 10/3): FP64 uses CUDA's pow (a few ulp from glibc's); FP32 uses
-// exp2(10/3 * log2(h)) on the special-function unit.
-__device__ inline double pow_10_3(double h) { return pow(h, 10.0 / 3.0); }
-__device__ inline float pow_10_3(float h) { return exp2f((10.0f / 3.0f) * __log2f(h)); }
-
 template <typename T>
 struct Phys {
   T dx, fn, depth_thresh, max_hflow, nodata, gdt;  // gdt = g*dt
   T g;
   T dxinv, gdt_fn2;  // 1/dx and g*dt*fn*fn (FP32 form only)
 };
-
-// Interior face flux with theta == 1 (src/kernels.cpp:51-92 / :101-142).
-// Cell 0 is west (x-face) or north (y-face) of the face; qa..qd are the
-// four cross-direction Qold values in the reference's summation order.
-template <typename T>
-__device__ inline T face_flux(T z0, T h0, T z1, T h1, T q0, T qa, T qb, T qc, T qd,
-                              const Phys<T>& ph) {
-  if (z0 == ph.nodata || z1 == ph.nodata) return T(0);
-  T y0 = z0 + h0, y1 = z1 + h1;
-  T dh = y0 - y1;
-  T Sf = -dh / ph.dx;
-  T hflow = gmaxT(y0, y1) - gmaxT(z0, z1);
-  hflow = gmaxT(hflow, T(0));
-  hflow = gminT(hflow, ph.max_hflow);
-  T Q = T(0);
-  if (hflow > ph.depth_thresh) {
-    T q_avg = (qa + qb + qc + qd) / T(4);
-    T qvect = sqrt(q0 * q0 + q_avg * q_avg);
-    // theta*q0 + 0.5*(1-theta)*(qup+qdown) with theta == 1 is q0 + 0.
-    T numerator = (q0 + T(0)) - (ph.gdt * hflow * Sf);
-    T denominator = T(1) + ph.gdt * hflow * ph.fn * ph.fn * fabs(qvect) / pow_10_3(hflow);
-    Q = numerator / denominator * ph.dx;
-    if (Q * dh < T(0)) {
-      numerator = q0 - (ph.gdt * hflow * Sf);
-      Q = numerator / denominator * ph.dx;
-    }
-  }
-  return Q;
-}
 
 // FREE edges (src/kernels.cpp:154-248).  West also needs the cell east of
 // the edge cell.
@@ -509,54 +463,77 @@ __device__ inline void update_cells(float (&hn)[4], const float (&qw)[4], const 
   }
 }
 
-// Persistent grid: block b processes tiles b, b + gridDim.x, ...; a tile is
-// WY strips stacked along y (warp w owns strip sy = tile_y*WY + w of column
-// strip sx).  Warps whose strip lies wholly inside the grid in x take a path
-// without the per-column edge tests.
-template <typename T, int WY, int MINB>
-__global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
+// ------------------------------------------------------------ one strip
+// Per-step values of one grid, derived from its control block at the start of
+// the step.
+template <typename T>
+struct StepScal {
+  double t, dt;
+  bool mass, rain_on;
+  int parity;
+  T rain_depth, dtT, dAT, dxinvT, dt_dA;
+  Phys<T> ph;
+};
+
+// src/kernels.cpp:36-43: dt from the previous state's Hmax; plus the step's
+// constants of the face law, rain and depth update.
+template <typename T>
+__device__ inline void step_scalars(const StepParams& p, double t, double hmax_prev, double rate,
+                                    double next_mass, int parity, StepScal<T>& s) {
+  const double dt = (hmax_prev > p.depth_thresh) ? p.cfl * p.dx / sqrt(p.g * hmax_prev)
+                                                 : p.init_tstep;
+  s.t = t;
+  s.dt = dt;
+  s.mass = p.mass_int > 0.0 && (t + dt >= next_mass);
+  s.rain_on = rate > 0.0;  // src/kernels.cpp:356
+  s.parity = parity;
+  s.rain_depth = T(rate * dt);
+  s.dtT = T(dt);
+  s.dAT = T(p.dA);
+  s.dxinvT = T(p.dxinv);
+  s.dt_dA = T(dt / p.dA);
+  s.ph.dx = T(p.dx);
+  s.ph.fn = T(p.fpn);
+  s.ph.depth_thresh = T(p.depth_thresh);
+  s.ph.max_hflow = T(p.max_hflow);
+  s.ph.nodata = T(p.nodata);
+  s.ph.g = T(p.g);
+  s.ph.gdt = T(p.g * dt);  // (g*dt) rounded once, as the reference's left-to-right product does
+  s.ph.dxinv = T(1.0 / p.dx);
+  s.ph.gdt_fn2 = T(p.g * dt * p.fpn * p.fpn);
+}
+
+// What one lane carries out of its strips: the max depth over its valid
+// cells (state precision; exact) and, at mass-report steps, its volume and
+// flooded-area sums.
+template <typename T>
+struct LaneAcc {
+  T m_cell;
+  bool any_cell;
+  double v, a;
+};
+
+// One step of strip (sx, sy) of one grid by one warp: the strip's OWN
+// columns and R rows, streamed through the warp's stage ring (`ring`, `bar`;
+// `kglob` = stages the warp has consumed so far, its position in the ring).
+// Warps whose strip lies wholly inside the grid in x take a path without the
+// per-column edge tests.  Returns false after a wait time-out, with the
+// copies in flight drained and the grid's status flagged.
+template <typename T>
+__device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>& sc, int sx,
+                                          int sy, unsigned char (*ring)[4][kRowBytes],
+                                          uint64_t* bar, int& kglob, LaneAcc<T>& acc) {
   constexpr int N = Lanes<T>::N;
   constexpr int OWN = 30 * N;
   static_assert(32 * N * sizeof(T) == kRowBytes, "one 16-byte vector per lane");
-  __shared__ __align__(128) unsigned char s_ring[WY][kStages][4][kRowBytes];
-  __shared__ __align__(8) uint64_t s_bar[WY][kStages];
-  SimCtl* ctl = p.ctl;
-  if (*(volatile int*)&ctl->done) return;
-
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int parity = ctl->parity;
-  const double t = ctl->t;
-  const double hmax_prev = ctl->hmax;
-  // src/kernels.cpp:36-43
-  const double dt = (hmax_prev > p.depth_thresh) ? p.cfl * p.dx / sqrt(p.g * hmax_prev)
-                                                 : p.init_tstep;
-  const bool mass = p.mass_int > 0.0 && (t + dt >= ctl->next_mass);
-  const double rate = ctl->rain_rate;
-  const bool rain_on = rate > 0.0;  // src/kernels.cpp:356
-  const T rain_depth = T(rate * dt);
-  const T dtT = T(dt), dAT = T(p.dA), dxinvT = T(p.dxinv), dt_dA = T(dt / p.dA);
-
-  Phys<T> ph;
-  ph.dx = T(p.dx);
-  ph.fn = T(p.fpn);
-  ph.depth_thresh = T(p.depth_thresh);
-  ph.max_hflow = T(p.max_hflow);
-  ph.nodata = T(p.nodata);
-  ph.g = T(p.g);
-  ph.gdt = T(p.g * dt);  // (g*dt) rounded once, as the reference's left-to-right product does
-  ph.dxinv = T(1.0 / p.dx);
-  ph.gdt_fn2 = T(p.g * dt * p.fpn * p.fpn);
-
-  const SeriesTable src_tb{p.src_type, p.src_value, p.src_off, p.src_times, p.src_vals,
-                           p.src_sorted};
-  const SeriesTable bc_tb{p.bc_type, p.bc_value, p.bc_off, p.bc_times, p.bc_vals, p.bc_sorted};
-  double m_loc = -DBL_MAX, v_loc = 0.0, a_loc = 0.0;
-  T m_cell = T(-FLT_MAX);  // running max of this lane's valid cells, state precision
-  bool any_cell = false;
-  bool failed = false;
-
   const int nx = p.nx, ny = p.ny, P = p.P;
+  const int parity = sc.parity;
+  const double t = sc.t, dt = sc.dt;
+  const bool mass = sc.mass, rain_on = sc.rain_on;
+  const T rain_depth = sc.rain_depth, dtT = sc.dtT, dAT = sc.dAT, dxinvT = sc.dxinvT,
+          dt_dA = sc.dt_dA;
+  const Phys<T> ph = sc.ph;
   const T* __restrict__ H = static_cast<const T*>(p.H[parity]);
   T* __restrict__ Hn = static_cast<T*>(p.H[parity ^ 1]);
   const T* __restrict__ Qx = static_cast<const T*>(p.Qx[parity]);
@@ -564,280 +541,349 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
   const T* __restrict__ Qy = static_cast<const T*>(p.Qy[parity]);
   T* __restrict__ Qyn = static_cast<T*>(p.Qy[parity ^ 1]);
   const T* __restrict__ Z = static_cast<const T*>(p.DEM);
+  bool failed = false;
+
+  const int x0 = sx * OWN;
+  const int cb = x0 - N + lane * N;          // first column of this lane
+  const long long wcol = (long long)x0 - N;  // first column of the warp's window
+  const bool own = lane >= 1 && lane <= 30;
+  const int j0 = sy * p.R;
+  const int j1 = min(j0 + p.R, ny);
+  const int strip = sy * p.nsx + sx;
+  int sp = p.spec_off[strip];
+  const int sp_end = p.spec_off[strip + 1];
+  // Rows to stream: j0-1 (H, DEM, Qx: the prologue) if j0 > 0, then j0..j1
+  // (all four; row ny only exists for Qy).
+  const int rfirst = j0 > 0 ? j0 - 1 : j0;
+  const int nload = j1 + 1 - rfirst;
+  // Lanes 0..3 each copy one array (H, DEM, Qx, Qy) of row rfirst+k into
+  // stage k; lane 0 also posts the expected byte count.  The prologue row
+  // j0-1 has no Qy; row ny has only Qy.
+  const T* const src_of[4] = {H, Z, Qx, Qy};
+  auto issue = [&](int k) {
+    const int r = rfirst + k;
+    const int slot = (kglob + k) % kStages;
+    const int a_lo = r < ny ? 0 : 3;
+    const int a_hi = r < j0 ? 3 : 4;
+    if (lane == 0) mbar_expect_tx(&bar[slot], (uint32_t)((a_hi - a_lo) * kRowBytes));
+    if (lane >= a_lo && lane < a_hi) {
+      fence_proxy_async();
+      bulk_g2s(&ring[slot][lane][0], src_of[lane] + (long long)r * P + wcol, kRowBytes,
+               &bar[slot]);
+    }
+  };
+  for (int k = 0; k < kStages && k < nload; k++) issue(k);
+  __syncwarp();
+  int kc = 0;  // next stage of this strip to consume
+  auto acquire = [&]() -> const unsigned char* {
+    const int q = kglob + kc;
+    if (!mbar_wait_warp(&bar[q % kStages], (uint32_t)((q / kStages) & 1))) return nullptr;
+    return &ring[q % kStages][0][0] + lane * 16;
+  };
+  auto release = [&]() {
+    __syncwarp();
+    if (kc + kStages < nload) issue(kc + kStages);
+    kc++;
+  };
+
+  T h[N], z[N], qxo[N], qyo[N], qyn[N];
+  T hp[N], zp[N], qxp[N];
+  if (j0 > 0) {
+    const unsigned char* st = acquire();
+    if (!st) failed = true;
+    if (!failed) {
+      lds_vec(st, hp);
+      lds_vec(st + kRowBytes, zp);
+      lds_vec(st + 2 * kRowBytes, qxp);
+      release();
+    }
+  }
+  if (!failed) {
+    const unsigned char* st = acquire();
+    if (!st) failed = true;
+    if (!failed) {
+      lds_vec(st, h);
+      lds_vec(st + kRowBytes, z);
+      lds_vec(st + 2 * kRowBytes, qxo);
+      lds_vec(st + 3 * kRowBytes, qyo);
+      release();
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        qxo[k] = qxo[k] * dxinvT;
+        qyo[k] = qyo[k] * dxinvT;
+      }
+    }
+  }
+  if (!failed) {
+    // North faces of row j0.
+    if (j0 == 0) {
+#pragma unroll
+      for (int k = 0; k < N; k++) qyn[k] = p.nf ? out_free(h[k], z[k], T(-1), ph.g, ph.dx, ph.nodata) : T(0);
+      if (own) {
+        if (cb + N <= nx) {
+          st_vec(Qyn + cb, qyn);
+        } else {
+#pragma unroll
+          for (int k = 0; k < N; k++)
+            if (cb + k < nx) Qyn[cb + k] = qyn[k];
+        }
+      }
+    } else {
+      // The south faces of row j0-1, by the same code (row_faces) that the
+      // strip above uses to compute and store them, so both strips see the
+      // same flux through their common edge, bit for bit, in either
+      // precision.  The west faces it also returns are not needed here.
+#pragma unroll
+      for (int k = 0; k < N; k++) qxp[k] = qxp[k] * dxinvT;
+      const T qxpR = __shfl_down_sync(0xffffffffu, qxp[0], 1);
+      const T qxoR = __shfl_down_sync(0xffffffffu, qxo[0], 1);
+      T qw_unused[N];
+      row_faces(hp, zp, h, z, qxp, qxo, qyo, qyo, T(0), T(0), T(0), T(0), qxpR, qxoR, true, ph,
+                qw_unused, qyn);
+    }
+  }
+
+  auto rows = [&](auto edge_tag) {
+    constexpr bool kEdge = decltype(edge_tag)::value;
+#pragma unroll kRowUnroll
+    for (int j = j0; j < j1; j++) {
+      const bool has_next = (j + 1 < ny);
+      T hN[N], zN[N], qxoN[N], qyoN[N];
+      {
+        const unsigned char* st = acquire();
+        if (!st) {
+          failed = true;
+          return;
+        }
+        lds_vec(st + 3 * kRowBytes, qyoN);
+        if (has_next) {
+          lds_vec(st, hN);
+          lds_vec(st + kRowBytes, zN);
+          lds_vec(st + 2 * kRowBytes, qxoN);
+        } else {
+#pragma unroll
+          for (int k = 0; k < N; k++) hN[k] = zN[k] = qxoN[k] = T(0);
+        }
+        release();
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+          qyoN[k] = qyoN[k] * dxinvT;
+          qxoN[k] = qxoN[k] * dxinvT;
+        }
+      }
+      // Neighbours across lanes.
+      const T hL = __shfl_up_sync(0xffffffffu, h[N - 1], 1);
+      const T zL = __shfl_up_sync(0xffffffffu, z[N - 1], 1);
+      const T qyoL = __shfl_up_sync(0xffffffffu, qyo[N - 1], 1);
+      const T qyoNL = __shfl_up_sync(0xffffffffu, qyoN[N - 1], 1);
+      const T qxoR = __shfl_down_sync(0xffffffffu, qxo[0], 1);
+      const T qxoNR = __shfl_down_sync(0xffffffffu, qxoN[0], 1);
+
+      // Faces of the row: interior law everywhere, then the edges.
+      T qw[N], qs[N];
+      row_faces(h, z, hN, zN, qxo, qxoN, qyo, qyoN, hL, zL, qyoL, qyoNL, qxoR, qxoNR, has_next,
+                ph, qw, qs);
+      if (kEdge) {
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+          const int c = cb + k;
+          if (c == 0) qw[k] = p.wf ? west_free(h[0], z[0], h[1], z[1], ph.g, ph.dx, ph.nodata) : T(0);
+          else if (c >= nx) qw[k] = T(0);
+        }
+      }
+      if (!has_next) {
+#pragma unroll
+        for (int k = 0; k < N; k++) qs[k] = p.sf ? out_free(h[k], z[k], T(1), ph.g, ph.dx, ph.nodata) : T(0);
+      }
+      const T qwR = __shfl_down_sync(0xffffffffu, qw[0], 1);
+      // East face of every cell.
+      T qe[N];
+#pragma unroll
+      for (int k = 0; k < N; k++) qe[k] = (k < N - 1) ? qw[k + 1] : qwR;
+      T qe_last = T(0);
+      if (kEdge) {
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+          if (cb + k == nx - 1) {
+            qe[k] = p.ef ? out_free(h[k], z[k], T(1), ph.g, ph.dx, ph.nodata) : T(0);
+            qe_last = qe[k];
+          }
+        }
+      }
+      // Depth update of the owned cells.
+      T hn[N];
+#pragma unroll
+      for (int k = 0; k < N; k++) hn[k] = h[k];
+      const int sp_row = sp;
+      // Point sources (src/main.cpp:245-262), before rain and the update.
+      while (sp < sp_end && p.spec[sp].row == j) {
+        const SpecCell e = p.spec[sp];
+        if (own) {
+#pragma unroll
+          for (int k = 0; k < N; k++)
+            if (cb + k == e.col)
+              hn[k] = apply_sources(hn[k], e.s0, e.s1,
+                                    SeriesTable{p.src_type, p.src_value, p.src_off, p.src_times,
+                                                p.src_vals, p.src_sorted},
+                                    p.dx, p.dA, t, dt);
+        }
+        sp++;
+      }
+      update_cells(hn, qw, qe, qyn, qs, z, rain_on, rain_depth, dtT, dAT, dt_dA, ph.nodata);
+      // Point depth BCs (src/kernels.cpp:259-277), after the update.
+      for (int q = sp_row; q < sp; q++) {
+        const SpecCell e = p.spec[q];
+        if (own && e.bc >= 0) {
+          const T v = bc_depth<T>(e.bc,
+                                  SeriesTable{p.bc_type, p.bc_value, p.bc_off, p.bc_times,
+                                              p.bc_vals, p.bc_sorted},
+                                  t);
+#pragma unroll
+          for (int k = 0; k < N; k++)
+            if (cb + k == e.col) hn[k] = v;
+        }
+      }
+      if (own) {
+        const long long r = (long long)j * P + cb;
+        const long long rs = r + P;
+        if (!kEdge || cb + N <= nx) {
+          st_vec(Hn + r, hn);
+          st_vec(Qxn + r, qw);
+          st_vec(Qyn + rs, qs);
+        } else {
+#pragma unroll
+          for (int k = 0; k < N; k++) {
+            if (cb + k < nx) {
+              Hn[r + k] = hn[k];
+              Qxn[r + k] = qw[k];
+              Qyn[rs + k] = qs[k];
+            }
+          }
+        }
+        if (kEdge && cb <= nx - 1 && nx - 1 < cb + N) Qxn[(long long)j * P + nx] = qe_last;
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+          if (!kEdge || cb + k < nx) {
+            if (z[k] != ph.nodata) {
+              acc.any_cell = true;
+              if (hn[k] > acc.m_cell) acc.m_cell = hn[k];
+            }
+            if (mass) {
+              const double hv = (double)hn[k];
+              acc.v += hv * p.dA;
+              if (hv > 0.01) acc.a += p.dA;
+            }
+          }
+        }
+      }
+      // Advance one row.
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        h[k] = hN[k];
+        z[k] = zN[k];
+        qxo[k] = qxoN[k];
+        qyo[k] = qyoN[k];
+        qyn[k] = qs[k];
+      }
+    }
+  };
+  if (!failed) {
+#if AF_EDGE_SPLIT
+    const bool interior = (x0 > 0) && (x0 + OWN < nx);
+    if (interior) rows(BoolC<false>());
+    else rows(BoolC<true>());
+#else
+    rows(BoolC<true>());
+#endif
+  }
+  if (failed) {
+    // Drain the copies still in flight into this warp's stages (bounded),
+    // then flag the control block so the loop stops with an error.
+    const int issued = min(nload, kc + kStages);
+    for (int k = kc; k < issued; k++)
+      mbar_wait_warp(&bar[(kglob + k) % kStages], (uint32_t)(((kglob + k) / kStages) & 1));
+    if (lane == 0) atomicExch(&p.ctl->status, 2);
+  }
+  kglob += nload;
+  return !failed;
+}
+
+// Folds a finished step into the grid's control block (one thread): the new
+// Hmax, t += dt (src/main.cpp:287), the mass report (:291-304), the next
+// step's rain rate, and the loop test of :227.  Returns whether this grid's
+// loop stops here.
+__device__ inline bool fold_step(const StepParams& p, SimCtl* ctl, double t, double dt, int parity,
+                                 bool mass, double vol, double area) {
+  const unsigned long long acc = atomicExch(&ctl->hmax_acc, ord_encode(-DBL_MAX));
+  const double hmax = ord_decode(acc);
+  const double t_new = t + dt;  // src/main.cpp:287
+  const long long step_new = ctl->step + 1;
+  ctl->hmax = hmax;
+  ctl->t = t_new;
+  ctl->dt_last = dt;
+  ctl->step = step_new;
+  ctl->parity = parity ^ 1;
+  if (mass) {  // src/main.cpp:291-304
+    const int k = ctl->mass_count;
+    if (k < ctl->mass_cap) {
+      p.mass_series[3 * k] = t_new;
+      p.mass_series[3 * k + 1] = vol;
+      p.mass_series[3 * k + 2] = area;
+      ctl->mass_count = k + 1;
+    }
+    ctl->next_mass += p.mass_int;
+  }
+  ctl->rain_rate = p.n_rain > 0 ? interp_series(p.rain_times, p.rain_rates, p.n_rain, 0.0, t_new,
+                                                p.rain_sorted != 0)
+                                : 0.0;
+  // A non-positive or non-finite dt (a diverged state) would stall time:
+  // stop the loop and report it instead.
+  const bool bad = !(dt > 0.0) || !(t_new < 1.0e300) || !(hmax == hmax) ||
+                   *(volatile int*)&ctl->status != 0;
+  if (bad) ctl->status = 1;
+  const bool done = bad || !(t_new < ctl->t_stop) || step_new >= ctl->step_stop;
+  ctl->done = done;
+  ctl->arrive = 0u;
+  return done;
+}
+
+// ------------------------------------------------------- single grid
+// Persistent grid: block b processes tiles b, b + gridDim.x, ...; a tile is
+// WY strips stacked along y (warp w owns strip sy = tile_y*WY + w of column
+// strip sx).  The last block to finish folds the step.
+template <typename T, int WY, int MINB>
+__global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
+  __shared__ __align__(128) unsigned char s_ring[WY][kStages][4][kRowBytes];
+  __shared__ __align__(8) uint64_t s_bar[WY][kStages];
+  SimCtl* ctl = p.ctl;
+  if (*(volatile int*)&ctl->done) return;
+
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  StepScal<T> sc;
+  step_scalars(p, ctl->t, ctl->hmax, ctl->rain_rate, ctl->next_mass, ctl->parity, sc);
+  const bool mass = sc.mass;
   uint64_t* bar = s_bar[warp];
   if (lane == 0) {
     for (int s = 0; s < kStages; s++) mbar_init(&bar[s], 1);
     fence_mbar_init();
   }
   __syncwarp();
-  int kglob = 0;  // stages this warp has consumed so far (position in its ring)
+  int kglob = 0;
+  LaneAcc<T> acc{T(-FLT_MAX), false, 0.0, 0.0};
   const int tiles_y = (p.nsy + WY - 1) / WY;
   const int ntiles = p.nsx * tiles_y;
-
-  for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int sx = tile % p.nsx;
     const int sy = (tile / p.nsx) * WY + warp;
     if (sy >= p.nsy) continue;
-
-    const int x0 = sx * OWN;
-    const int cb = x0 - N + lane * N;          // first column of this lane
-    const long long wcol = (long long)x0 - N;  // first column of the warp's window
-    const bool own = lane >= 1 && lane <= 30;
-    const int j0 = sy * p.R;
-    const int j1 = min(j0 + p.R, ny);
-    const int strip = sy * p.nsx + sx;
-    int sp = p.spec_off[strip];
-    const int sp_end = p.spec_off[strip + 1];
-    // Rows to stream: j0-1 (H, DEM, Qx: the prologue) if j0 > 0, then j0..j1
-    // (all four; row ny only exists for Qy).
-    const int rfirst = j0 > 0 ? j0 - 1 : j0;
-    const int nload = j1 + 1 - rfirst;
-    // Lanes 0..3 each copy one array (H, DEM, Qx, Qy) of row rfirst+k into
-    // stage k; lane 0 also posts the expected byte count.  The prologue row
-    // j0-1 has no Qy; row ny has only Qy.
-    const T* const src_of[4] = {H, Z, Qx, Qy};
-    auto issue = [&](int k) {
-      const int r = rfirst + k;
-      const int slot = (kglob + k) % kStages;
-      const int a_lo = r < ny ? 0 : 3;
-      const int a_hi = r < j0 ? 3 : 4;
-      if (lane == 0) mbar_expect_tx(&bar[slot], (uint32_t)((a_hi - a_lo) * kRowBytes));
-      if (lane >= a_lo && lane < a_hi) {
-        fence_proxy_async();
-        bulk_g2s(&s_ring[warp][slot][lane][0], src_of[lane] + (long long)r * P + wcol, kRowBytes,
-                 &bar[slot]);
-      }
-    };
-    for (int k = 0; k < kStages && k < nload; k++) issue(k);
-    __syncwarp();
-    int kc = 0;  // next stage of this strip to consume
-    auto acquire = [&]() -> const unsigned char* {
-      const int q = kglob + kc;
-      if (!mbar_wait_warp(&bar[q % kStages], (uint32_t)((q / kStages) & 1))) return nullptr;
-      return &s_ring[warp][q % kStages][0][0] + lane * 16;
-    };
-    auto release = [&]() {
-      __syncwarp();
-      if (kc + kStages < nload) issue(kc + kStages);
-      kc++;
-    };
-
-    T h[N], z[N], qxo[N], qyo[N], qyn[N];
-    T hp[N], zp[N], qxp[N];
-    if (j0 > 0) {
-      const unsigned char* st = acquire();
-      if (!st) failed = true;
-      if (!failed) {
-        lds_vec(st, hp);
-        lds_vec(st + kRowBytes, zp);
-        lds_vec(st + 2 * kRowBytes, qxp);
-        release();
-      }
-    }
-    if (!failed) {
-      const unsigned char* st = acquire();
-      if (!st) failed = true;
-      if (!failed) {
-        lds_vec(st, h);
-        lds_vec(st + kRowBytes, z);
-        lds_vec(st + 2 * kRowBytes, qxo);
-        lds_vec(st + 3 * kRowBytes, qyo);
-        release();
-#pragma unroll
-        for (int k = 0; k < N; k++) {
-          qxo[k] = qxo[k] * dxinvT;
-          qyo[k] = qyo[k] * dxinvT;
-        }
-      }
-    }
-    if (!failed) {
-      // North faces of row j0.
-      if (j0 == 0) {
-#pragma unroll
-        for (int k = 0; k < N; k++) qyn[k] = p.nf ? out_free(h[k], z[k], T(-1), ph.g, ph.dx, ph.nodata) : T(0);
-        if (own) {
-          if (cb + N <= nx) {
-            st_vec(Qyn + cb, qyn);
-          } else {
-#pragma unroll
-            for (int k = 0; k < N; k++)
-              if (cb + k < nx) Qyn[cb + k] = qyn[k];
-          }
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < N; k++) qxp[k] = qxp[k] * dxinvT;
-        const T qxpR = __shfl_down_sync(0xffffffffu, qxp[0], 1);
-        const T qxoR = __shfl_down_sync(0xffffffffu, qxo[0], 1);
-#pragma unroll
-        for (int k = 0; k < N; k++) {
-          const T qb = (k < N - 1) ? qxp[k + 1] : qxpR;
-          const T qd = (k < N - 1) ? qxo[k + 1] : qxoR;
-          qyn[k] = face_flux(zp[k], hp[k], z[k], h[k], qyo[k], qxp[k], qb, qxo[k], qd, ph);
-        }
-      }
-    }
-
-    auto rows = [&](auto edge_tag) {
-      constexpr bool kEdge = decltype(edge_tag)::value;
-#pragma unroll kRowUnroll
-      for (int j = j0; j < j1; j++) {
-        const bool has_next = (j + 1 < ny);
-        T hN[N], zN[N], qxoN[N], qyoN[N];
-        {
-          const unsigned char* st = acquire();
-          if (!st) {
-            failed = true;
-            return;
-          }
-          lds_vec(st + 3 * kRowBytes, qyoN);
-          if (has_next) {
-            lds_vec(st, hN);
-            lds_vec(st + kRowBytes, zN);
-            lds_vec(st + 2 * kRowBytes, qxoN);
-          } else {
-#pragma unroll
-            for (int k = 0; k < N; k++) hN[k] = zN[k] = qxoN[k] = T(0);
-          }
-          release();
-#pragma unroll
-          for (int k = 0; k < N; k++) {
-            qyoN[k] = qyoN[k] * dxinvT;
-            qxoN[k] = qxoN[k] * dxinvT;
-          }
-        }
-        // Neighbours across lanes.
-        const T hL = __shfl_up_sync(0xffffffffu, h[N - 1], 1);
-        const T zL = __shfl_up_sync(0xffffffffu, z[N - 1], 1);
-        const T qyoL = __shfl_up_sync(0xffffffffu, qyo[N - 1], 1);
-        const T qyoNL = __shfl_up_sync(0xffffffffu, qyoN[N - 1], 1);
-        const T qxoR = __shfl_down_sync(0xffffffffu, qxo[0], 1);
-        const T qxoNR = __shfl_down_sync(0xffffffffu, qxoN[0], 1);
-
-        // Faces of the row: interior law everywhere, then the edges.
-        T qw[N], qs[N];
-        row_faces(h, z, hN, zN, qxo, qxoN, qyo, qyoN, hL, zL, qyoL, qyoNL, qxoR, qxoNR, has_next,
-                  ph, qw, qs);
-        if (kEdge) {
-#pragma unroll
-          for (int k = 0; k < N; k++) {
-            const int c = cb + k;
-            if (c == 0) qw[k] = p.wf ? west_free(h[0], z[0], h[1], z[1], ph.g, ph.dx, ph.nodata) : T(0);
-            else if (c >= nx) qw[k] = T(0);
-          }
-        }
-        if (!has_next) {
-#pragma unroll
-          for (int k = 0; k < N; k++) qs[k] = p.sf ? out_free(h[k], z[k], T(1), ph.g, ph.dx, ph.nodata) : T(0);
-        }
-        const T qwR = __shfl_down_sync(0xffffffffu, qw[0], 1);
-        // East face of every cell.
-        T qe[N];
-#pragma unroll
-        for (int k = 0; k < N; k++) qe[k] = (k < N - 1) ? qw[k + 1] : qwR;
-        T qe_last = T(0);
-        if (kEdge) {
-#pragma unroll
-          for (int k = 0; k < N; k++) {
-            if (cb + k == nx - 1) {
-              qe[k] = p.ef ? out_free(h[k], z[k], T(1), ph.g, ph.dx, ph.nodata) : T(0);
-              qe_last = qe[k];
-            }
-          }
-        }
-        // Depth update of the owned cells.
-        T hn[N];
-#pragma unroll
-        for (int k = 0; k < N; k++) hn[k] = h[k];
-        const int sp_row = sp;
-        // Point sources (src/main.cpp:245-262), before rain and the update.
-        while (sp < sp_end && p.spec[sp].row == j) {
-          const SpecCell e = p.spec[sp];
-          if (own) {
-#pragma unroll
-            for (int k = 0; k < N; k++)
-              if (cb + k == e.col) hn[k] = apply_sources(hn[k], e.s0, e.s1, src_tb, p.dx, p.dA, t, dt);
-          }
-          sp++;
-        }
-        update_cells(hn, qw, qe, qyn, qs, z, rain_on, rain_depth, dtT, dAT, dt_dA, ph.nodata);
-        // Point depth BCs (src/kernels.cpp:259-277), after the update.
-        for (int q = sp_row; q < sp; q++) {
-          const SpecCell e = p.spec[q];
-          if (own && e.bc >= 0) {
-            const T v = bc_depth<T>(e.bc, bc_tb, t);
-#pragma unroll
-            for (int k = 0; k < N; k++)
-              if (cb + k == e.col) hn[k] = v;
-          }
-        }
-        if (own) {
-          const long long r = (long long)j * P + cb;
-          const long long rs = r + P;
-          if (!kEdge || cb + N <= nx) {
-            st_vec(Hn + r, hn);
-            st_vec(Qxn + r, qw);
-            st_vec(Qyn + rs, qs);
-          } else {
-#pragma unroll
-            for (int k = 0; k < N; k++) {
-              if (cb + k < nx) {
-                Hn[r + k] = hn[k];
-                Qxn[r + k] = qw[k];
-                Qyn[rs + k] = qs[k];
-              }
-            }
-          }
-          if (kEdge && cb <= nx - 1 && nx - 1 < cb + N) Qxn[(long long)j * P + nx] = qe_last;
-#pragma unroll
-          for (int k = 0; k < N; k++) {
-            if (!kEdge || cb + k < nx) {
-              if (z[k] != ph.nodata) {
-                any_cell = true;
-                if (hn[k] > m_cell) m_cell = hn[k];
-              }
-              if (mass) {
-                const double hv = (double)hn[k];
-                v_loc += hv * p.dA;
-                if (hv > 0.01) a_loc += p.dA;
-              }
-            }
-          }
-        }
-        // Advance one row.
-#pragma unroll
-        for (int k = 0; k < N; k++) {
-          h[k] = hN[k];
-          z[k] = zN[k];
-          qxo[k] = qxoN[k];
-          qyo[k] = qyoN[k];
-          qyn[k] = qs[k];
-        }
-      }
-    };
-    if (!failed) {
-#if AF_EDGE_SPLIT
-      const bool interior = (x0 > 0) && (x0 + OWN < nx);
-      if (interior) rows(BoolC<false>());
-      else rows(BoolC<true>());
-#else
-      rows(BoolC<true>());
-#endif
-    }
-    if (failed) {
-      // Drain the copies still in flight into this warp's stages (bounded),
-      // then flag the control block so the loop stops with an error.
-      const int issued = min(nload, kc + kStages);
-      for (int k = kc; k < issued; k++)
-        mbar_wait_warp(&bar[(kglob + k) % kStages], (uint32_t)(((kglob + k) / kStages) & 1));
-      if (lane == 0) atomicExch(&ctl->status, 2);
-    }
-    kglob += nload;
+    if (!run_strip<T>(p, sc, sx, sy, s_ring[warp], bar, kglob, acc)) break;
   }
 
   // A valid cell's depth is finite (NaN never wins a comparison), and in
   // FP64 m_cell is exact; a lane with no valid cell keeps the identity.
-  if (any_cell && (double)m_cell > m_loc) m_loc = (double)m_cell;
+  double m_loc = -DBL_MAX, v_loc = acc.v, a_loc = acc.a;
+  if (acc.any_cell && (double)acc.m_cell > m_loc) m_loc = (double)acc.m_cell;
 
   // ----- block reductions: Hmax, and volume/area at mass-report steps -----
   __shared__ double s_m[WY], s_v[WY], s_a[WY];
@@ -901,38 +947,233 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    const unsigned long long acc = atomicExch(&ctl->hmax_acc, ord_encode(-DBL_MAX));
-    const double hmax = ord_decode(acc);
-    const double t_new = t + dt;  // src/main.cpp:287
-    const long long step_new = ctl->step + 1;
-    ctl->hmax = hmax;
-    ctl->t = t_new;
-    ctl->dt_last = dt;
-    ctl->step = step_new;
-    ctl->parity = parity ^ 1;
-    if (mass) {  // src/main.cpp:291-304
-      const int k = ctl->mass_count;
-      if (k < ctl->mass_cap) {
-        p.mass_series[3 * k] = t_new;
-        p.mass_series[3 * k + 1] = r_v[0];
-        p.mass_series[3 * k + 2] = r_a[0];
-        ctl->mass_count = k + 1;
-      }
-      ctl->next_mass += p.mass_int;
-    }
-    ctl->rain_rate = p.n_rain > 0 ? interp_series(p.rain_times, p.rain_rates, p.n_rain, 0.0, t_new,
-                                                  p.rain_sorted != 0)
-                                  : 0.0;
-    // A non-positive or non-finite dt (a diverged state) would stall time:
-    // stop the loop and report it instead.
-    const bool bad = !(dt > 0.0) || !(t_new < 1.0e300) || !(hmax == hmax) ||
-                     *(volatile int*)&ctl->status != 0;
-    if (bad) ctl->status = 1;
-    const int done = bad || !(t_new < ctl->t_stop) || step_new >= ctl->step_stop;
-    ctl->done = done;
-    ctl->arrive = 0u;
+    const bool done = fold_step(p, ctl, sc.t, sc.dt, sc.parity, mass, r_v[0], r_a[0]);
     __threadfence();
     if (p.use_cond) cudaGraphSetConditional(p.cond, done ? 0u : 1u);
+  }
+}
+
+// ------------------------------------------------------------ batches
+// A batch advances many independent grids ("scenarios": each with its own
+// size, parameters, forcing, dt and time) by one step each per launch.  The
+// work units of a launch are the strips of the active scenarios, numbered
+// scenario after scenario (u0[a] = first unit of active scenario a); warp w
+// of the persistent grid takes units w, w + W, ... (W = warps in the grid).
+// The warp that finishes the last strip of a scenario folds that scenario's
+// step (one arrival counter per scenario, no waiting); the last block of the
+// launch rebuilds the active list for the next launch and sets the loop
+// condition.  A scenario's results do not depend on which other scenarios
+// share the batch: every face and cell is computed by the same code, Hmax is
+// an exact max, and its volume partials are summed per strip in strip order.
+constexpr int kMaxSlots = 1024;
+
+struct BatchTab {
+  int nmember;                // slots in the batch (written by the host)
+  int member[kMaxSlots];
+  int nact;                   // scenarios stepped by the coming launch
+  int units;                  // their strips
+  int act[kMaxSlots];         // their slots
+  int u0[kMaxSlots + 1];      // first unit of each; u0[nact] = units
+};
+
+struct BatchCtl {
+  long long step;       // batch steps taken
+  long long step_stop;  // the loop stops when step reaches this,
+  unsigned int arrive;  // (blocks finished in this step)
+  int completed;        // or, with stop_on_done, once a scenario has finished,
+  int stop_on_done;
+  int done;             // or when nothing is active or the host asks for attention
+  int status;           // nonzero: a wait timed out; the batch's state is invalid
+};
+
+struct BatchParams {
+  const StepParams* scen;          // per slot
+  BatchTab* tab;
+  BatchCtl* bctl;
+  const volatile int* attention;   // host memory mapped into the device; may be null
+  cudaGraphConditionalHandle cond;
+  int use_cond;
+};
+
+// The active list: members whose time is below their stop time and whose
+// state is sound, with their strip offsets.  One warp.
+__device__ inline void batch_compact(const BatchParams& bp) {
+  BatchTab* tab = bp.tab;
+  const int lane = threadIdx.x & 31;
+  const int nm = tab->nmember;
+  int nact = 0, units = 0;
+  for (int base = 0; base < nm; base += 32) {
+    const int i = base + lane;
+    int slot = -1, nu = 0;
+    bool act = false;
+    if (i < nm) {
+      slot = tab->member[i];
+      const StepParams* sp = &bp.scen[slot];
+      const SimCtl* c = sp->ctl;
+      act = __ldcg(&c->status) == 0 && __ldcg(&c->t) < __ldcg(&c->t_stop) &&
+            __ldcg(&c->step) < __ldcg(&c->step_stop);
+      nu = sp->nsx * sp->nsy;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, act);
+    int x = act ? nu : 0;  // inclusive scan of the active lanes' strip counts
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (act) {
+      const int pos = nact + __popc(m & ((1u << lane) - 1u));
+      tab->act[pos] = slot;
+      tab->u0[pos] = units + x - nu;
+    }
+    nact += __popc(m);
+    units += __shfl_sync(0xffffffffu, x, 31);
+  }
+  if (lane == 0) {
+    tab->nact = nact;
+    tab->units = units;
+    tab->u0[nact] = units;
+  }
+}
+
+// Sum of the per-strip volume/area partials of one grid in a fixed order
+// (lane l takes strips l, l+32, ..., Neumaier-compensated; then the lanes in
+// order), by one warp; every lane gets the result.
+__device__ inline void warp_fold_partials(const double* part, int n, double& vol, double& area) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0, c = 0.0, a = 0.0;
+  for (int k = lane; k < n; k += 32) {
+    kahan_add(s, c, __ldcg(&part[3 * k]));
+    a += __ldcg(&part[3 * k + 2]);
+  }
+  double S = 0.0, C = 0.0, A = 0.0;
+  for (int l = 0; l < 32; l++) {
+    kahan_add(S, C, __shfl_sync(0xffffffffu, s, l));
+    C += __shfl_sync(0xffffffffu, c, l);
+    A += __shfl_sync(0xffffffffu, a, l);
+  }
+  vol = S + C;
+  area = A;
+}
+
+template <typename T, int WY, int MINB>
+__global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams bp) {
+  __shared__ __align__(128) unsigned char s_ring[WY][kStages][4][kRowBytes];
+  __shared__ __align__(8) uint64_t s_bar[WY][kStages];
+  __shared__ __align__(16) StepParams s_par[WY];
+  __shared__ __align__(16) StepScal<T> s_sc[WY];
+  __shared__ int s_fail;
+  __shared__ bool s_last;
+  BatchCtl* bctl = bp.bctl;
+  if (*(volatile int*)&bctl->done) return;
+  const BatchTab* tab = bp.tab;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  uint64_t* bar = s_bar[warp];
+  if (threadIdx.x == 0) s_fail = 0;
+  if (lane == 0) {
+    for (int s = 0; s < kStages; s++) mbar_init(&bar[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int kglob = 0;
+  const int units = tab->units;
+  const int nact = tab->nact;
+  const int W = gridDim.x * WY;
+  int a = 0;     // active-scenario index of the current unit (only grows)
+  int cur = -1;  // slot whose parameters are in s_par[warp] and s_sc[warp]
+  StepScal<T>& sc = s_sc[warp];
+  bool ok = true;
+  for (int u = blockIdx.x * WY + warp; u < units; u += W) {
+    for (;;) {  // u0 is increasing: count the entries past `a` that are <= u
+      const int idx = a + 1 + lane;
+      const bool le = idx < nact && tab->u0[idx] <= u;
+      const unsigned m = __ballot_sync(0xffffffffu, le);
+      a += __popc(m);
+      if (m != 0xffffffffu) break;
+    }
+    const int slot = tab->act[a];
+    StepParams& p = s_par[warp];
+    if (slot != cur) {
+      __syncwarp();
+      const int* src = reinterpret_cast<const int*>(&bp.scen[slot]);
+      int* dst = reinterpret_cast<int*>(&p);
+      for (int i = lane; i < (int)(sizeof(StepParams) / 4); i += 32) dst[i] = src[i];
+      __syncwarp();
+      cur = slot;
+      if (lane == 0) {
+        const SimCtl* c = p.ctl;
+        step_scalars(p, c->t, c->hmax, c->rain_rate, c->next_mass, c->parity, sc);
+      }
+      __syncwarp();
+    }
+    const int k = u - tab->u0[a];
+    const int nunits = p.nsx * p.nsy;
+    LaneAcc<T> acc{T(-FLT_MAX), false, 0.0, 0.0};
+    ok = run_strip<T>(p, sc, k % p.nsx, k / p.nsx, s_ring[warp], bar, kglob, acc);
+    double m = (acc.any_cell) ? (double)acc.m_cell : -DBL_MAX;
+    m = warp_maxd(m);
+    double v = 0.0, ar = 0.0;
+    if (sc.mass) {
+      v = warp_sum(acc.v);
+      ar = warp_sum(acc.a);
+    }
+    unsigned prev = 0;
+    if (lane == 0) {
+      SimCtl* ctl = p.ctl;
+      if (m > -DBL_MAX) atomicMax(&ctl->hmax_acc, ord_encode(m));
+      if (sc.mass) {
+        p.partials[3 * k] = v;
+        p.partials[3 * k + 1] = 0.0;
+        p.partials[3 * k + 2] = ar;
+      }
+      __threadfence();
+      prev = atomicAdd(&ctl->arrive, 1u);
+    }
+    prev = __shfl_sync(0xffffffffu, prev, 0);
+    if (prev == (unsigned)nunits - 1u) {  // this warp finished the scenario's step
+      __threadfence();
+      double vol = 0.0, area = 0.0;
+      if (sc.mass) warp_fold_partials(p.partials, nunits, vol, area);
+      if (lane == 0) {
+        if (fold_step(p, p.ctl, sc.t, sc.dt, sc.parity, sc.mass, vol, area))
+          atomicAdd(&bctl->completed, 1);
+        __threadfence();  // the fold is visible before this block's arrival
+      }
+      __syncwarp();
+    }
+    if (!ok) {
+      // A wait timed out: the batch's state is no longer consistent (other
+      // strips of this step will never be counted), so stop it.
+      if (lane == 0) atomicExch(&s_fail, 1);
+      break;
+    }
+  }
+
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_fail) atomicExch(&bctl->status, 1);
+    __threadfence();
+    const unsigned prev = atomicAdd(&bctl->arrive, 1u);
+    s_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (warp == 0) {
+    batch_compact(bp);
+    __syncwarp();
+    if (lane == 0) {
+      const long long step_new = bctl->step + 1;
+      bctl->step = step_new;
+      bctl->arrive = 0u;
+      const bool attn = bp.attention != nullptr && *bp.attention != 0;
+      const bool stop = tab->nact == 0 || step_new >= bctl->step_stop ||
+                        *(volatile int*)&bctl->status != 0 ||
+                        (bctl->stop_on_done && *(volatile int*)&bctl->completed > 0) || attn;
+      bctl->done = stop;
+      __threadfence();
+      if (bp.use_cond) cudaGraphSetConditional(bp.cond, stop ? 0u : 1u);
+    }
   }
 }
 
@@ -946,5 +1187,7 @@ constexpr int kStepVariants = 5;
 constexpr StepVariant kStepVariant[kStepVariants] = {{1, 16}, {1, 12}, {1, 20}, {4, 4}, {2, 8}};
 const void* step_kernel_f64(int variant);
 const void* step_kernel_f32(int variant);
+const void* batch_kernel_f64(int variant);
+const void* batch_kernel_f32(int variant);
 
 }  // namespace af

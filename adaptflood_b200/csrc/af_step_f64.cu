@@ -13,4 +13,13 @@ const void* step_kernel_f64(int variant) {
     default: return (const void*)&k_step<double, 1, 16>;
   }
 }
+const void* batch_kernel_f64(int variant) {
+  switch (variant) {
+    case 1: return (const void*)&k_batch_step<double, 1, 12>;
+    case 2: return (const void*)&k_batch_step<double, 1, 20>;
+    case 3: return (const void*)&k_batch_step<double, 4, 4>;
+    case 4: return (const void*)&k_batch_step<double, 2, 8>;
+    default: return (const void*)&k_batch_step<double, 1, 16>;
+  }
+}
 }  // namespace af

@@ -371,6 +371,18 @@ def config4(seed: int = 4, count: int = 256, lo: int = 256, hi: int = 2048,
     return [ensemble_case(rng, seed * 100003 + k, lo, hi, sim_time) for k in range(count)]
 
 
+def config5(seed: int = 5, count: int = 32, lo: int = 128, hi: int = 4096,
+            sim_time=(600.0, 3600.0)) -> List[Case]:
+    """Served-loop requests: grids log-uniform in [lo^2, hi^2] cells with the
+    ensemble generator, each with its own sim_time drawn from U(sim_time)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        st = float(rng.uniform(*sim_time))
+        out.append(ensemble_case(rng, seed * 100019 + k, lo, hi, sim_time=st))
+    return out
+
+
 def small_case(nx: int, ny: int, seed: int, dx: float = 10.0, free: Sequence[bool] = (1, 1, 1, 1),
                n_qfix: int = 1, n_qvar: int = 1, n_hfix: int = 0, n_hvar: int = 0,
                n_free_pts: int = 0, dup_sources: bool = False, rain: bool = False,

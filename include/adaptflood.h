@@ -1,6 +1,6 @@
 /* adaptflood.h -- C ABI of the B200-native AdaptFlood local-inertial time step.
  *
- * Two layers share this header:
+ * Three layers share this header (plus the input-file reader):
  *
  * 1. The drop-in layer (af_update_qs ... af_fill).  One entry point per
  *    function of the reference's src/kernels.hpp plus the three pieces of
@@ -19,6 +19,10 @@
  *    time step with device-resident dt, time and hydrograph interpolation, in
  *    FP64 (results within 1e-9 m of the reference) or FP32 state with FP64
  *    time, interpolation and volume accumulation.
+ *
+ * 3. The batch layer (af_batch_*): many grids of uneven sizes with their own
+ *    dt stepped together by one persistent, graph-launched kernel, placed in
+ *    one device arena and admitted by memory footprint (continuous batching).
  *
  * Point boundaries: the reference's src/main.cpp:256-260 scatter and
  * src/kernels.cpp:261-274 overwrite run one thread per boundary and race when
@@ -219,7 +223,100 @@ int af_sim_volume(af_sim* s, double* vol, double* area);
  * (src/main.cpp:291-304): up to cap entries of (t, vol, area). */
 int af_sim_mass_series(af_sim* s, double* t, double* vol, double* area, int cap, int* n);
 
-/* ============================================== 3. input files (host) == */
+/* ======================================================= 3. batch layer == */
+
+/* No counterpart in the reference, which runs one grid per process: a batch
+ * steps many independent grids ("scenarios": own size, parameters, forcing,
+ * adaptive dt and stop time) together, one persistent kernel per batch step
+ * inside one CUDA graph, each scenario advancing by its own dt exactly as
+ * af_sim would step it alone (bit for bit: a scenario's results do not depend
+ * on the other members).  Scenarios start at t = 0 (src/main.cpp:197) and
+ * stop once t >= t_stop (the loop test of src/main.cpp:227).
+ *
+ * Device memory: af_batch_create takes one arena of arena_bytes; every
+ * scenario's state and tables are placed inside it.  af_batch_add refuses a
+ * scenario whose footprint (af_batch_footprint) does not fit in the free
+ * arena space with AF_ENOMEM and changes nothing, so a caller admits work by
+ * HBM footprint and retries after af_batch_remove frees space.  At most
+ * AF_BATCH_MAX_SLOTS scenarios are members at once.
+ *
+ * One host thread drives a batch.  af_batch_launch enqueues batch steps
+ * without waiting; af_batch_sync waits and refreshes the per-slot status that
+ * af_batch_slot_status reports.  While a launch is in flight, af_batch_add
+ * uploads on a separate copy stream (the scenario joins at the next launch),
+ * af_batch_remove defers the release to the next af_batch_sync, and
+ * af_batch_get_state works for scenarios that had finished at the last sync. */
+#define AF_BATCH_MAX_SLOTS 1024
+
+typedef struct af_batch af_batch;
+
+/* precision: AF_PREC_F32 or AF_PREC_F64.  variant: launch shape of the batch
+ * step kernel (0..4, warps per block x resident blocks per SM), -1 = the
+ * default. */
+int af_batch_create(int precision, int device, uint64_t arena_bytes, int variant,
+                    af_batch** out);
+int af_batch_destroy(af_batch* b);
+
+/* Strip height (rows) used for scenarios of a size class, class =
+ * floor(log2(nx*ny)) (0..31).  Applies to scenarios added afterwards; the
+ * autotuner sets these.  Results do not depend on the strip height except for
+ * the rounding of the volume/area diagnostics. */
+int af_batch_size_class(int nx, int ny);
+int af_batch_set_rows(af_batch* b, int size_class, int rows);
+int af_batch_get_rows(const af_batch* b, int size_class);
+
+/* Arena bytes a scenario would take (fields, tables, reduction and mass-series
+ * space) with the batch's precision and current strip heights. */
+int af_batch_footprint(const af_batch* b, const af_case_desc* c, const af_forcing_desc* f,
+                       double t_stop, uint64_t* bytes);
+/* Admits a scenario from HOST arrays (dem, optional h0 as af_sim_create);
+ * *slot receives its slot id.  AF_ENOMEM: no room in the arena or no free
+ * slot (nothing changed). */
+int af_batch_add(af_batch* b, const af_case_desc* c, const af_forcing_desc* f, const double* dem,
+                 const double* h0, double t_stop, int* slot);
+int af_batch_remove(af_batch* b, int slot);
+
+/* Enqueues batch steps until no member is active, max_steps batch steps have
+ * run, (stop_on_done != 0) a scenario has finished, or af_batch_attention is
+ * called; does not wait. */
+int af_batch_launch(af_batch* b, int64_t max_steps, int stop_on_done);
+/* Asks the launch in flight to stop after its current batch step (sets a
+ * flag in host memory mapped into the device; safe from any thread). */
+int af_batch_attention(af_batch* b);
+/* 1 when no launch is in flight or it has finished (af_batch_sync will not
+ * wait), 0 while it runs; never waits. */
+int af_batch_query(af_batch* b);
+/* Waits for the launch; AF_ESTATE if the batch's state is invalid. */
+int af_batch_sync(af_batch* b);
+/* af_batch_launch(b, max_steps, 0) + af_batch_sync. */
+int af_batch_run(af_batch* b, int64_t max_steps, int64_t* batch_steps);
+
+/* Status of a slot as of the last sync.  *state: 0 running, 1 finished
+ * (t >= t_stop), -1 stopped on a bad state (non-finite or non-positive dt). */
+int af_batch_slot_status(const af_batch* b, int slot, double* t, double* dt_last, double* hmax,
+                         int64_t* steps, int* state);
+/* State of a slot in the reference layout, HOST FP64 arrays (as
+ * af_sim_get_state); any pointer may be NULL. */
+int af_batch_get_state(af_batch* b, int slot, double* H, double* Qx, double* Qy);
+int af_batch_mass_series(af_batch* b, int slot, double* t, double* vol, double* area, int cap,
+                         int* n);
+int af_batch_info(const af_batch* b, int* members, int64_t* batch_steps, uint64_t* arena_bytes,
+                  uint64_t* arena_used, uint64_t* arena_largest_free);
+/* The device stream batch launches run on (a cudaStream_t). */
+void* af_batch_stream(af_batch* b);
+
+/* The batch's arena planner on its own (host only, no device memory): best-fit
+ * placement of 256-byte-aligned blocks in a range of `bytes`, coalescing
+ * neighbours on release.  A caller can plan admissions with it. */
+typedef struct af_arena af_arena;
+int af_arena_create(uint64_t bytes, af_arena** out);
+int af_arena_destroy(af_arena* a);
+/* AF_ENOMEM when no free block holds `bytes` (nothing changes). */
+int af_arena_alloc(af_arena* a, uint64_t bytes, uint64_t* off);
+int af_arena_free(af_arena* a, uint64_t off);
+int af_arena_stats(const af_arena* a, uint64_t* used, uint64_t* largest_free, int* blocks);
+
+/* ============================================== 4. input files (host) == */
 
 /* A case parsed from a .par file and the files it names, with the
  * reference's parsing rules (src/io.cpp:9-296). */
