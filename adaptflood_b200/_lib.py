@@ -96,6 +96,7 @@ _SIGS = {
     "af_batch_query": (_i, [_vp]),
     "af_batch_sync": (_i, [_vp]),
     "af_batch_run": (_i, [_vp, _i64, _vp]),
+    "af_batch_set_balance": (_i, [_vp, _i]),
     "af_batch_slot_status": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "af_batch_get_state": (_i, [_vp, _i, _vp, _vp, _vp]),
     "af_batch_mass_series": (_i, [_vp, _i, _vp, _vp, _vp, _i, _vp]),

@@ -73,6 +73,11 @@ class Batch:
     def set_rows(self, cls: int, rows: int) -> None:
         _lib.check(self.lib.af_batch_set_rows(self.h, int(cls), int(rows)), "af_batch_set_rows")
 
+    def set_balance(self, strips_per_warp: int) -> None:
+        """Load-adaptive strip height target (0 = off); see af_batch_set_balance."""
+        _lib.check(self.lib.af_batch_set_balance(self.h, int(strips_per_warp)),
+                   "af_batch_set_balance")
+
     def rows(self, cls: int) -> int:
         return self.lib.af_batch_get_rows(self.h, int(cls))
 

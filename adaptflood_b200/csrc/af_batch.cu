@@ -38,25 +38,6 @@
 
 namespace af {
 
-// Sets up one launch of the batch loop (one block of one warp): the step
-// limit, the active list, and the loop condition.
-__global__ void k_batch_begin(const BatchParams bp, long long max_steps, int stop_on_done) {
-  BatchCtl* b = bp.bctl;
-  batch_compact(bp);
-  __syncwarp();
-  if (threadIdx.x == 0) {
-    const long long s = b->step;
-    b->step_stop = (max_steps > (long long)0x3FFFFFFFFFFFFFFFLL - s) ? 0x3FFFFFFFFFFFFFFFLL
-                                                                     : s + max_steps;
-    b->completed = 0;
-    b->stop_on_done = stop_on_done;
-    b->arrive = 0u;
-    const int done = bp.tab->nact == 0 || max_steps <= 0 || b->status != 0;
-    b->done = done;
-    if (bp.use_cond) cudaGraphSetConditional(bp.cond, done ? 0u : 1u);
-  }
-}
-
 constexpr int kClasses = 32;  // size class = floor(log2(nx*ny))
 constexpr int kBatchMassCap = 1 << 16;
 
@@ -134,7 +115,9 @@ static Layout make_layout(const af_case_desc* c, const af_forcing_desc* f, doubl
   L.bc_sorted = put(no);
   L.rain_times = put(sizeof(double) * f->n_rain);
   L.rain_rates = put(sizeof(double) * f->n_rain);
-  const size_t nstrips = (size_t)L.nsx * L.nsy;
+  // Per-strip arrays are sized for one-row strips, so the strip height can
+  // change between launches without moving anything.
+  const size_t nstrips = (size_t)L.nsx * L.ny;
   L.spec_off = put(sizeof(int) * (nstrips + 1));
   L.spec = put(sizeof(SpecCell) * (size_t)(nf + no));  // at most one per source or BC
   L.partials = put(sizeof(double) * 3 * nstrips);
@@ -153,6 +136,9 @@ struct Slot {
   Layout L;
   af_case_desc c{};
   double t_stop = 0.0;
+  int cls = 0;                  // size class
+  std::vector<SpecCell> spec;   // special cells in (column strip, row, col) order
+  StepParams p{};               // the device copy's host image
 };
 
 struct Batch {
@@ -160,7 +146,7 @@ struct Batch {
   cudaStream_t st = nullptr, cst = nullptr;
   char* arena = nullptr;
   Arena plan;
-  StepParams* d_scen = nullptr;
+  BatchScen* d_scen = nullptr;
   SimCtl* d_ctl = nullptr;
   BatchTab* d_tab = nullptr;
   BatchCtl* d_bctl = nullptr;
@@ -178,6 +164,7 @@ struct Batch {
   bool use_cond = false;
   bool in_flight = false;
   bool members_dirty = true;
+  int balance = 6;  // strips per warp the load-adaptive strip height aims at (0: off)
   int hi_slot = 0;  // one past the highest slot ever used
   int rows[kClasses];
   std::vector<Slot> slots;
@@ -203,6 +190,12 @@ struct Batch {
 
   const void* kernel() const {
     return prec == AF_PREC_F64 ? batch_kernel_f64(variant) : batch_kernel_f32(variant);
+  }
+  const void* begin_kernel() const {
+    return prec == AF_PREC_F64 ? batch_begin_f64() : batch_begin_f32();
+  }
+  const void* fold_kernel() const {
+    return prec == AF_PREC_F64 ? batch_fold_f64() : batch_fold_f32();
   }
 };
 
@@ -236,9 +229,9 @@ static int build_graph(Batch& b) {
   int stop_on_done = 0;
   void* bargs[] = {&b.bp, &max_steps, &stop_on_done};
   cudaKernelNodeParams kb{};
-  kb.func = (void*)&k_batch_begin;
+  kb.func = const_cast<void*>(b.begin_kernel());
   kb.gridDim = dim3(1);
-  kb.blockDim = dim3(32);
+  kb.blockDim = dim3(kFoldThreads);
   kb.kernelParams = bargs;
   AF_CUDA(cudaGraphAddKernelNode(&b.begin_node, b.graph, nullptr, 0, &kb));
   cudaGraphNodeParams cp{};
@@ -249,14 +242,21 @@ static int build_graph(Batch& b) {
   cudaGraphNode_t cnode;
   AF_CUDA(cudaGraphAddNode(&cnode, b.graph, &b.begin_node, 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
+  // Body: the strips of every active scenario, then the fold.
   void* sargs[] = {&b.bp};
   cudaKernelNodeParams ks{};
   ks.func = const_cast<void*>(b.kernel());
   ks.gridDim = b.grid;
   ks.blockDim = b.block;
   ks.kernelParams = sargs;
-  cudaGraphNode_t snode;
+  cudaGraphNode_t snode, fnode;
   AF_CUDA(cudaGraphAddKernelNode(&snode, body, nullptr, 0, &ks));
+  cudaKernelNodeParams kf{};
+  kf.func = const_cast<void*>(b.fold_kernel());
+  kf.gridDim = dim3(1);
+  kf.blockDim = dim3(kFoldThreads);
+  kf.kernelParams = sargs;
+  AF_CUDA(cudaGraphAddKernelNode(&fnode, body, &snode, 1, &kf));
   AF_CUDA(cudaGraphInstantiate(&b.exec, b.graph, 0));
   return AF_OK;
 }
@@ -272,7 +272,9 @@ static int create(int precision, int device, uint64_t arena_bytes, int variant, 
   b->esize = precision == AF_PREC_F64 ? 8 : 4;
   b->N = 16 / b->esize;
   if (variant < 0) {
-    variant = 0;
+    // Default: 1 warp per block, 12 resident blocks per SM (168 registers, no
+    // spills; the 16-block shape spills scenario parameters held in registers).
+    variant = 1;
     if (const char* v = getenv("AF_BATCH_VARIANT")) variant = atoi(v);
   }
   if (variant < 0 || variant >= kStepVariants) return AF_EINVAL;
@@ -285,11 +287,11 @@ static int create(int precision, int device, uint64_t arena_bytes, int variant, 
   AF_CUDA(cudaStreamCreateWithFlags(&b->cst, cudaStreamNonBlocking));
   AF_TRY(alloc_dev((void**)&b->arena, arena_bytes));
   b->plan.reset(arena_bytes);
-  AF_TRY(alloc_dev((void**)&b->d_scen, sizeof(StepParams) * kMaxSlots));
+  AF_TRY(alloc_dev((void**)&b->d_scen, sizeof(BatchScen) * kMaxSlots));
   AF_TRY(alloc_dev((void**)&b->d_ctl, sizeof(SimCtl) * kMaxSlots));
   AF_TRY(alloc_dev((void**)&b->d_tab, sizeof(BatchTab)));
   AF_TRY(alloc_dev((void**)&b->d_bctl, sizeof(BatchCtl)));
-  AF_CUDA(cudaMemsetAsync(b->d_scen, 0, sizeof(StepParams) * kMaxSlots, b->st));
+  AF_CUDA(cudaMemsetAsync(b->d_scen, 0, sizeof(BatchScen) * kMaxSlots, b->st));
   AF_CUDA(cudaMemsetAsync(b->d_ctl, 0, sizeof(SimCtl) * kMaxSlots, b->st));
   AF_CUDA(cudaMemsetAsync(b->d_tab, 0, sizeof(BatchTab), b->st));
   AF_CUDA(cudaMemsetAsync(b->d_bctl, 0, sizeof(BatchCtl), b->st));
@@ -447,7 +449,7 @@ static int add(Batch& b, const af_case_desc* c, const af_forcing_desc* f, const 
   h.step_stop = 0x3FFFFFFFFFFFFFFFLL;
   h.hmax_acc = ord_encode(-DBL_MAX);
   h.mass_cap = L.mass_cap;
-  if (cudaMemcpyAsync(b.d_scen + slot, &p, sizeof(p), cudaMemcpyHostToDevice, b.cst) !=
+  if (cudaMemcpyAsync(&b.d_scen[slot].p, &p, sizeof(p), cudaMemcpyHostToDevice, b.cst) !=
           cudaSuccess ||
       cudaMemcpyAsync(b.d_ctl + slot, &h, sizeof(h), cudaMemcpyHostToDevice, b.cst) !=
           cudaSuccess)
@@ -470,6 +472,9 @@ static int add(Batch& b, const af_case_desc* c, const af_forcing_desc* f, const 
   s.L = L;
   s.c = *c;
   s.t_stop = t_stop;
+  s.cls = size_class((long long)c->nx * c->ny);
+  s.spec = std::move(tb.spec);
+  s.p = p;
   b.h_ctl[slot] = h;  // the mirror until the next sync (Hmax not yet read back)
   b.hi_slot = std::max(b.hi_slot, slot + 1);
   b.members_dirty = true;
@@ -477,9 +482,71 @@ static int add(Batch& b, const af_case_desc* c, const af_forcing_desc* f, const 
   return AF_OK;
 }
 
+static bool finished(const Batch& b, int slot);
+
+// Re-cuts a member into strips of R rows: the strip index of its special
+// cells (the cells themselves are in an order that does not depend on R) and
+// its parameters.  Results do not depend on R; only the volume diagnostics'
+// rounding does.  Stream-ordered before the next launch.
+static int set_slot_rows(Batch& b, int slot, int R) {
+  Slot& s = b.slots[slot];
+  const int own = 30 * b.N;
+  const int nsy = (s.L.ny + R - 1) / R;
+  const size_t nstrips = (size_t)s.L.nsx * nsy;
+  std::vector<int> off(nstrips + 1, 0);
+  for (const SpecCell& e : s.spec) off[(size_t)(e.col / own) * nsy + e.row / R + 1]++;
+  for (size_t k = 0; k < nstrips; k++) off[k + 1] += off[k];
+  char* base = b.arena + s.off;
+  AF_CUDA(cudaMemcpyAsync(base + s.L.spec_off, off.data(), off.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, b.st));
+  s.p.R = R;
+  s.p.nsy = nsy;
+  s.L.R = R;
+  s.L.nsy = nsy;
+  AF_CUDA(cudaMemcpyAsync(&b.d_scen[slot].p, &s.p, sizeof(StepParams), cudaMemcpyHostToDevice,
+                          b.st));
+  // Pageable sources: wait until the copies have left host memory.
+  AF_CUDA(cudaStreamSynchronize(b.st));
+  return AF_OK;
+}
+
+// Load-adaptive strip height: the tuned height of each member's size class,
+// lowered (in powers of two, to at least 2 rows) until the active members
+// give every warp of the persistent grid about `balance` strips, so the
+// steps near the end of a run, when few scenarios remain, keep the SMs busy.
+static int retile(Batch& b) {
+  if (b.balance <= 0) return AF_OK;
+  std::vector<int> act;
+  for (int k = 0; k < b.hi_slot; k++)
+    if (b.slots[k].state == 1 && !finished(b, k)) act.push_back(k);
+  if (act.empty()) return AF_OK;
+  const long long target = (long long)b.balance * b.grid.x * b.WY;
+  auto units = [&](int Rcap) {
+    long long u = 0;
+    for (int k : act) {
+      const Slot& s = b.slots[k];
+      const int R = std::min(b.rows[s.cls], Rcap);
+      u += (long long)s.L.nsx * ((s.L.ny + R - 1) / R);
+    }
+    return u;
+  };
+  int Rload = 2;
+  for (int R = 4096; R >= 2; R >>= 1)
+    if (units(R) >= target) {
+      Rload = R;
+      break;
+    }
+  for (int k : act) {
+    const int R = std::max(1, std::min(b.rows[b.slots[k].cls], Rload));
+    if (R != b.slots[k].L.R) AF_TRY(set_slot_rows(b, k, R));
+  }
+  return AF_OK;
+}
+
 static int launch(Batch& b, long long max_steps, int stop_on_done) {
   if (b.in_flight) return AF_ESTATE;
   AF_CUDA(cudaSetDevice(b.device));
+  AF_TRY(retile(b));
   if (b.members_dirty) {
     int n = 0;
     for (int k = 0; k < b.hi_slot; k++)
@@ -493,22 +560,25 @@ static int launch(Batch& b, long long max_steps, int stop_on_done) {
   if (b.use_cond) {
     void* bargs[] = {&b.bp, &max_steps, &stop_on_done};
     cudaKernelNodeParams kb{};
-    kb.func = (void*)&k_batch_begin;
+    kb.func = const_cast<void*>(b.begin_kernel());
     kb.gridDim = dim3(1);
-    kb.blockDim = dim3(32);
+    kb.blockDim = dim3(kFoldThreads);
     kb.kernelParams = bargs;
     AF_CUDA(cudaGraphExecKernelNodeSetParams(b.exec, b.begin_node, &kb));
     AF_CUDA(cudaGraphLaunch(b.exec, b.st));
   } else {
     // Host-driven launches, in batches of 64 steps with a status check.
-    k_batch_begin<<<1, 32, 0, b.st>>>(b.bp, max_steps, stop_on_done);
     BatchParams p = b.bp;
+    void* bargs[] = {&p, &max_steps, &stop_on_done};
+    AF_CUDA(cudaLaunchKernel(b.begin_kernel(), dim3(1), dim3(kFoldThreads), bargs, 0, b.st));
     void* args[] = {&p};
     long long left = max_steps;
     while (left > 0) {
       const long long n = left < 64 ? left : 64;
-      for (long long k = 0; k < n; k++)
+      for (long long k = 0; k < n; k++) {
         AF_CUDA(cudaLaunchKernel(b.kernel(), b.grid, b.block, args, 0, b.st));
+        AF_CUDA(cudaLaunchKernel(b.fold_kernel(), dim3(1), dim3(kFoldThreads), args, 0, b.st));
+      }
       left -= n;
       AF_CUDA(cudaMemcpyAsync(b.h_bctl, b.d_bctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, b.st));
       AF_CUDA(cudaStreamSynchronize(b.st));
@@ -686,10 +756,28 @@ int af_batch_run(af_batch* h, int64_t max_steps, int64_t* batch_steps) {
   if (!h) return AF_EINVAL;
   Batch& b = *h->b;
   const long long before = b.h_bctl->step;
-  AF_TRY(af::launch(b, max_steps, 0));
-  const int rc = af::sync(b);
+  int rc = AF_OK;
+  // With the load-adaptive strip height, each launch ends when a scenario
+  // finishes, so the next one is cut for the members that remain.
+  for (;;) {
+    const long long left = max_steps - (b.h_bctl->step - before);
+    if (left <= 0) break;
+    AF_TRY(af::launch(b, left, b.balance > 0));
+    rc = af::sync(b);
+    if (rc != AF_OK) break;
+    bool any = false;
+    for (int k = 0; k < b.hi_slot && !any; k++)
+      any = b.slots[k].state == 1 && !af::finished(b, k);
+    if (!any || b.balance <= 0) break;
+  }
   if (batch_steps) *batch_steps = b.h_bctl->step - before;
   return rc;
+}
+
+int af_batch_set_balance(af_batch* h, int strips_per_warp) {
+  if (!h || strips_per_warp < 0) return AF_EINVAL;
+  h->b->balance = strips_per_warp;
+  return AF_OK;
 }
 
 int af_batch_slot_status(const af_batch* h, int slot, double* t, double* dt_last, double* hmax,

@@ -97,7 +97,7 @@ void build_tables(const af_case_desc* c, const af_forcing_desc* f, int own, int 
   }
   // ---- special cells
   struct Ent {
-    long long key;
+    long long strip;
     SpecCell e;
   };
   std::vector<Ent> ents;
@@ -124,8 +124,8 @@ void build_tables(const af_case_desc* c, const af_forcing_desc* f, int own, int 
       e.s1 = s1;
       e.bc = bc;
       int sx = e.col / own, sy = e.row / R;
-      long long strip = (long long)sy * nsx + sx;
-      ents.push_back({(strip << 40) | ((long long)e.row << 20) | 0, e});
+      long long strip = (long long)sx * nsy + sy;  // column-major: order independent of R
+      ents.push_back({strip, e});
     };
     // merge the sorted source cells with the sorted bc cells
     while (k < order.size() || qb < bc_of.size()) {
@@ -142,15 +142,18 @@ void build_tables(const af_case_desc* c, const af_forcing_desc* f, int own, int 
       emit(cell, s0, (int)k, bc);
     }
   }
+  // Sorted by (strip, row, col); with column-major strip ids this is the
+  // order (column strip, row, col) whatever the strip height.
   std::stable_sort(ents.begin(), ents.end(), [](const Ent& a, const Ent& b) {
-    if (a.key != b.key) return a.key < b.key;
+    if (a.strip != b.strip) return a.strip < b.strip;
+    if (a.e.row != b.e.row) return a.e.row < b.e.row;
     return a.e.col < b.e.col;
   });
   const long long nstrips = (long long)nsx * nsy;
   t.spec_off.assign(nstrips + 1, 0);
   t.spec.clear();
   for (auto& e : ents) {
-    t.spec_off[(e.key >> 40) + 1]++;
+    t.spec_off[e.strip + 1]++;
     t.spec.push_back(e.e);
   }
   for (long long q = 0; q < nstrips; q++) t.spec_off[q + 1] += t.spec_off[q];

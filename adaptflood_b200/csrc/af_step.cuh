@@ -94,7 +94,7 @@ struct StepParams {
   const double* rain_times;
   const double* rain_rates;
   int n_rain, rain_sorted;
-  // special cells per strip (CSR over strip id = sy*nsx + sx, sorted by row, col)
+  // special cells per strip (CSR over strip id = sx*nsy + sy, sorted by row, col)
   const int* spec_off;
   const SpecCell* spec;
   SimCtl* ctl;
@@ -475,13 +475,15 @@ struct StepScal {
   Phys<T> ph;
 };
 
-// src/kernels.cpp:36-43: dt from the previous state's Hmax; plus the step's
-// constants of the face law, rain and depth update.
+// src/kernels.cpp:36-43: dt from the previous state's Hmax.
+__device__ inline double step_dt(const StepParams& p, double hmax_prev) {
+  return (hmax_prev > p.depth_thresh) ? p.cfl * p.dx / sqrt(p.g * hmax_prev) : p.init_tstep;
+}
+
+// The step's constants of the face law, rain and depth update for dt.
 template <typename T>
-__device__ inline void step_scalars(const StepParams& p, double t, double hmax_prev, double rate,
+__device__ inline void fill_scalars(const StepParams& p, double t, double dt, double rate,
                                     double next_mass, int parity, StepScal<T>& s) {
-  const double dt = (hmax_prev > p.depth_thresh) ? p.cfl * p.dx / sqrt(p.g * hmax_prev)
-                                                 : p.init_tstep;
   s.t = t;
   s.dt = dt;
   s.mass = p.mass_int > 0.0 && (t + dt >= next_mass);
@@ -501,6 +503,12 @@ __device__ inline void step_scalars(const StepParams& p, double t, double hmax_p
   s.ph.gdt = T(p.g * dt);  // (g*dt) rounded once, as the reference's left-to-right product does
   s.ph.dxinv = T(1.0 / p.dx);
   s.ph.gdt_fn2 = T(p.g * dt * p.fpn * p.fpn);
+}
+
+template <typename T>
+__device__ inline void step_scalars(const StepParams& p, double t, double hmax_prev, double rate,
+                                    double next_mass, int parity, StepScal<T>& s) {
+  fill_scalars(p, t, step_dt(p, hmax_prev), rate, next_mass, parity, s);
 }
 
 // What one lane carries out of its strips: the max depth over its valid
@@ -549,7 +557,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
   const bool own = lane >= 1 && lane <= 30;
   const int j0 = sy * p.R;
   const int j1 = min(j0 + p.R, ny);
-  const int strip = sy * p.nsx + sx;
+  const int strip = sx * p.nsy + sy;  // column-major: the special-cell order is R-independent
   int sp = p.spec_off[strip];
   const int sp_end = p.spec_off[strip + 1];
   // Rows to stream: j0-1 (H, DEM, Qx: the prologue) if j0 > 0, then j0..j1
@@ -955,22 +963,36 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
 
 // ------------------------------------------------------------ batches
 // A batch advances many independent grids ("scenarios": each with its own
-// size, parameters, forcing, dt and time) by one step each per launch.  The
-// work units of a launch are the strips of the active scenarios, numbered
-// scenario after scenario (u0[a] = first unit of active scenario a); warp w
-// of the persistent grid takes units w, w + W, ... (W = warps in the grid).
-// The warp that finishes the last strip of a scenario folds that scenario's
-// step (one arrival counter per scenario, no waiting); the last block of the
-// launch rebuilds the active list for the next launch and sets the loop
-// condition.  A scenario's results do not depend on which other scenarios
-// share the batch: every face and cell is computed by the same code, Hmax is
-// an exact max, and its volume partials are summed per strip in strip order.
+// size, parameters, forcing, dt and time) by one step each per batch step.
+// A batch step is two kernels in the body of the graph's while loop:
+//   k_batch_step: the strips of every active scenario.  Units are numbered
+//     scenario after scenario (u0[a] = first unit of active scenario a); warp
+//     w of the persistent grid takes units w, w + W, ...; within a scenario,
+//     unit k is strip (k % nsx, k / nsx), so the warps running at the same
+//     time read adjacent 512-byte segments of the same rows.  A unit ends
+//     with a fire-and-forget atomicMax of its Hmax and, at mass-report steps,
+//     a store of its volume partials; nothing waits.
+//   k_batch_fold (one block): folds every active scenario's step (a thread
+//     per scenario; a warp per volume sum at mass-report steps), writes the
+//     scenario's next dt, time and parity beside its parameters, rebuilds the
+//     active list when a scenario has finished, and sets the loop condition.
+// A scenario's results do not depend on which other scenarios share the
+// batch: every face and cell is computed by the same code, Hmax is an exact
+// max, and its volume partials are summed per strip in strip order.
 constexpr int kMaxSlots = 1024;
+constexpr int kFoldThreads = 1024;  // one block of the fold and begin kernels
+
+// Per slot: the scenario's parameters and its coming step.
+struct BatchScen {
+  StepParams p;
+  double t, dt, rate, next_mass;  // written by the begin and fold kernels
+  int parity, pad;
+};
 
 struct BatchTab {
   int nmember;                // slots in the batch (written by the host)
   int member[kMaxSlots];
-  int nact;                   // scenarios stepped by the coming launch
+  int nact;                   // scenarios stepped by the coming step
   int units;                  // their strips
   int act[kMaxSlots];         // their slots
   int u0[kMaxSlots + 1];      // first unit of each; u0[nact] = units
@@ -979,7 +1001,6 @@ struct BatchTab {
 struct BatchCtl {
   long long step;       // batch steps taken
   long long step_stop;  // the loop stops when step reaches this,
-  unsigned int arrive;  // (blocks finished in this step)
   int completed;        // or, with stop_on_done, once a scenario has finished,
   int stop_on_done;
   int done;             // or when nothing is active or the host asks for attention
@@ -987,7 +1008,7 @@ struct BatchCtl {
 };
 
 struct BatchParams {
-  const StepParams* scen;          // per slot
+  BatchScen* scen;                 // per slot
   BatchTab* tab;
   BatchCtl* bctl;
   const volatile int* attention;   // host memory mapped into the device; may be null
@@ -1008,7 +1029,7 @@ __device__ inline void batch_compact(const BatchParams& bp) {
     bool act = false;
     if (i < nm) {
       slot = tab->member[i];
-      const StepParams* sp = &bp.scen[slot];
+      const StepParams* sp = &bp.scen[slot].p;
       const SimCtl* c = sp->ctl;
       act = __ldcg(&c->status) == 0 && __ldcg(&c->t) < __ldcg(&c->t_stop) &&
             __ldcg(&c->step) < __ldcg(&c->step_stop);
@@ -1035,6 +1056,41 @@ __device__ inline void batch_compact(const BatchParams& bp) {
   }
 }
 
+// The coming step of one scenario, from its control block.
+__device__ inline void batch_next(BatchScen* s) {
+  const SimCtl* c = s->p.ctl;
+  s->t = c->t;
+  s->dt = step_dt(s->p, c->hmax);
+  s->rate = c->rain_rate;
+  s->next_mass = c->next_mass;
+  s->parity = c->parity;
+}
+
+// Sets up one launch of the batch loop: the step limit, the active list,
+// each active scenario's coming step, and the loop condition.
+template <typename T>
+__global__ void __launch_bounds__(kFoldThreads) k_batch_begin(const BatchParams bp,
+                                                              long long max_steps,
+                                                              int stop_on_done) {
+  BatchCtl* b = bp.bctl;
+  const BatchTab* tab = bp.tab;
+  if (threadIdx.x < 32) batch_compact(bp);
+  __syncthreads();
+  const int nact = tab->nact;
+  for (int a = threadIdx.x; a < nact; a += blockDim.x) batch_next(&bp.scen[tab->act[a]]);
+  if (threadIdx.x == 0) {
+    const long long s = b->step;
+    b->step_stop = (max_steps > (long long)0x3FFFFFFFFFFFFFFFLL - s) ? 0x3FFFFFFFFFFFFFFFLL
+                                                                     : s + max_steps;
+    b->completed = 0;
+    b->stop_on_done = stop_on_done;
+    const int done = nact == 0 || max_steps <= 0 || b->status != 0;
+    b->done = done;
+    __threadfence();
+    if (bp.use_cond) cudaGraphSetConditional(bp.cond, done ? 0u : 1u);
+  }
+}
+
 // Sum of the per-strip volume/area partials of one grid in a fixed order
 // (lane l takes strips l, l+32, ..., Neumaier-compensated; then the lanes in
 // order), by one warp; every lane gets the result.
@@ -1042,8 +1098,8 @@ __device__ inline void warp_fold_partials(const double* part, int n, double& vol
   const int lane = threadIdx.x & 31;
   double s = 0.0, c = 0.0, a = 0.0;
   for (int k = lane; k < n; k += 32) {
-    kahan_add(s, c, __ldcg(&part[3 * k]));
-    a += __ldcg(&part[3 * k + 2]);
+    kahan_add(s, c, part[3 * k]);
+    a += part[3 * k + 2];
   }
   double S = 0.0, C = 0.0, A = 0.0;
   for (int l = 0; l < 32; l++) {
@@ -1055,34 +1111,80 @@ __device__ inline void warp_fold_partials(const double* part, int n, double& vol
   area = A;
 }
 
+// Folds one batch step (one block): see the section comment.
+template <typename T>
+__global__ void __launch_bounds__(kFoldThreads) k_batch_fold(const BatchParams bp) {
+  __shared__ double s_vol[kMaxSlots], s_area[kMaxSlots];
+  BatchCtl* b = bp.bctl;
+  const BatchTab* tab = bp.tab;
+  const int nact = tab->nact;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int a = warp; a < nact; a += nwarps) {  // volume sums of the reporting scenarios
+    const BatchScen* s = &bp.scen[tab->act[a]];
+    if (s->p.mass_int > 0.0 && s->t + s->dt >= s->next_mass) {
+      double v, ar;
+      warp_fold_partials(s->p.partials, s->p.nsx * s->p.nsy, v, ar);
+      if (lane == 0) {
+        s_vol[a] = v;
+        s_area[a] = ar;
+      }
+    }
+  }
+  __syncthreads();
+  int done = 0;
+  for (int a = threadIdx.x; a < nact; a += blockDim.x) {
+    BatchScen* s = &bp.scen[tab->act[a]];
+    const bool mass = s->p.mass_int > 0.0 && s->t + s->dt >= s->next_mass;
+    if (fold_step(s->p, s->p.ctl, s->t, s->dt, s->parity, mass, mass ? s_vol[a] : 0.0,
+                  mass ? s_area[a] : 0.0))
+      done++;
+    else
+      batch_next(s);
+  }
+  const int ndone = __syncthreads_count(done);
+  if (ndone > 0) {  // the active list changes only when a scenario finishes
+    __threadfence();
+    if (threadIdx.x < 32) batch_compact(bp);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const long long step_new = b->step + 1;
+    b->step = step_new;
+    b->completed += ndone;
+    const bool attn = bp.attention != nullptr && *bp.attention != 0;
+    const bool stop = tab->nact == 0 || step_new >= b->step_stop ||
+                      *(volatile int*)&b->status != 0 || (b->stop_on_done && b->completed > 0) ||
+                      attn;
+    b->done = stop;
+    __threadfence();
+    if (bp.use_cond) cudaGraphSetConditional(bp.cond, stop ? 0u : 1u);
+  }
+}
+
 template <typename T, int WY, int MINB>
 __global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams bp) {
   __shared__ __align__(128) unsigned char s_ring[WY][kStages][4][kRowBytes];
   __shared__ __align__(8) uint64_t s_bar[WY][kStages];
-  __shared__ __align__(16) StepParams s_par[WY];
+  __shared__ __align__(16) BatchScen s_scen[WY];
   __shared__ __align__(16) StepScal<T> s_sc[WY];
-  __shared__ int s_fail;
-  __shared__ bool s_last;
-  BatchCtl* bctl = bp.bctl;
-  if (*(volatile int*)&bctl->done) return;
+  if (*(volatile int*)&bp.bctl->done) return;
   const BatchTab* tab = bp.tab;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   uint64_t* bar = s_bar[warp];
-  if (threadIdx.x == 0) s_fail = 0;
   if (lane == 0) {
     for (int s = 0; s < kStages; s++) mbar_init(&bar[s], 1);
     fence_mbar_init();
   }
-  __syncthreads();
+  __syncwarp();
   int kglob = 0;
   const int units = tab->units;
   const int nact = tab->nact;
   const int W = gridDim.x * WY;
   int a = 0;     // active-scenario index of the current unit (only grows)
-  int cur = -1;  // slot whose parameters are in s_par[warp] and s_sc[warp]
+  int cur = -1;  // slot whose record is in s_scen[warp] and s_sc[warp]
+  const StepParams& p = s_scen[warp].p;
   StepScal<T>& sc = s_sc[warp];
-  bool ok = true;
   for (int u = blockIdx.x * WY + warp; u < units; u += W) {
     for (;;) {  // u0 is increasing: count the entries past `a` that are <= u
       const int idx = a + 1 + lane;
@@ -1092,24 +1194,22 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams 
       if (m != 0xffffffffu) break;
     }
     const int slot = tab->act[a];
-    StepParams& p = s_par[warp];
-    if (slot != cur) {
+    if (slot != cur) {  // one parallel load of the scenario's record
       __syncwarp();
       const int* src = reinterpret_cast<const int*>(&bp.scen[slot]);
-      int* dst = reinterpret_cast<int*>(&p);
-      for (int i = lane; i < (int)(sizeof(StepParams) / 4); i += 32) dst[i] = src[i];
+      int* dst = reinterpret_cast<int*>(&s_scen[warp]);
+      for (int i = lane; i < (int)(sizeof(BatchScen) / 4); i += 32) dst[i] = src[i];
       __syncwarp();
       cur = slot;
       if (lane == 0) {
-        const SimCtl* c = p.ctl;
-        step_scalars(p, c->t, c->hmax, c->rain_rate, c->next_mass, c->parity, sc);
+        const BatchScen& r = s_scen[warp];
+        fill_scalars(p, r.t, r.dt, r.rate, r.next_mass, r.parity, sc);
       }
       __syncwarp();
     }
     const int k = u - tab->u0[a];
-    const int nunits = p.nsx * p.nsy;
     LaneAcc<T> acc{T(-FLT_MAX), false, 0.0, 0.0};
-    ok = run_strip<T>(p, sc, k % p.nsx, k / p.nsx, s_ring[warp], bar, kglob, acc);
+    const bool ok = run_strip<T>(p, sc, k % p.nsx, k / p.nsx, s_ring[warp], bar, kglob, acc);
     double m = (acc.any_cell) ? (double)acc.m_cell : -DBL_MAX;
     m = warp_maxd(m);
     double v = 0.0, ar = 0.0;
@@ -1117,62 +1217,18 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams 
       v = warp_sum(acc.v);
       ar = warp_sum(acc.a);
     }
-    unsigned prev = 0;
     if (lane == 0) {
-      SimCtl* ctl = p.ctl;
-      if (m > -DBL_MAX) atomicMax(&ctl->hmax_acc, ord_encode(m));
+      if (m > -DBL_MAX) atomicMax(&p.ctl->hmax_acc, ord_encode(m));
       if (sc.mass) {
         p.partials[3 * k] = v;
         p.partials[3 * k + 1] = 0.0;
         p.partials[3 * k + 2] = ar;
       }
-      __threadfence();
-      prev = atomicAdd(&ctl->arrive, 1u);
-    }
-    prev = __shfl_sync(0xffffffffu, prev, 0);
-    if (prev == (unsigned)nunits - 1u) {  // this warp finished the scenario's step
-      __threadfence();
-      double vol = 0.0, area = 0.0;
-      if (sc.mass) warp_fold_partials(p.partials, nunits, vol, area);
-      if (lane == 0) {
-        if (fold_step(p, p.ctl, sc.t, sc.dt, sc.parity, sc.mass, vol, area))
-          atomicAdd(&bctl->completed, 1);
-        __threadfence();  // the fold is visible before this block's arrival
-      }
-      __syncwarp();
     }
     if (!ok) {
-      // A wait timed out: the batch's state is no longer consistent (other
-      // strips of this step will never be counted), so stop it.
-      if (lane == 0) atomicExch(&s_fail, 1);
+      // A wait timed out: this step's state is incomplete, so stop the batch.
+      if (lane == 0) atomicExch(&bp.bctl->status, 1);
       break;
-    }
-  }
-
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (s_fail) atomicExch(&bctl->status, 1);
-    __threadfence();
-    const unsigned prev = atomicAdd(&bctl->arrive, 1u);
-    s_last = (prev == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  if (warp == 0) {
-    batch_compact(bp);
-    __syncwarp();
-    if (lane == 0) {
-      const long long step_new = bctl->step + 1;
-      bctl->step = step_new;
-      bctl->arrive = 0u;
-      const bool attn = bp.attention != nullptr && *bp.attention != 0;
-      const bool stop = tab->nact == 0 || step_new >= bctl->step_stop ||
-                        *(volatile int*)&bctl->status != 0 ||
-                        (bctl->stop_on_done && *(volatile int*)&bctl->completed > 0) || attn;
-      bctl->done = stop;
-      __threadfence();
-      if (bp.use_cond) cudaGraphSetConditional(bp.cond, stop ? 0u : 1u);
     }
   }
 }
@@ -1189,5 +1245,11 @@ const void* step_kernel_f64(int variant);
 const void* step_kernel_f32(int variant);
 const void* batch_kernel_f64(int variant);
 const void* batch_kernel_f32(int variant);
+// Begin and fold kernels of the batch loop (one block of kFoldThreads),
+// compiled beside the step kernels of the same precision.
+const void* batch_begin_f64();
+const void* batch_begin_f32();
+const void* batch_fold_f64();
+const void* batch_fold_f32();
 
 }  // namespace af

@@ -22,4 +22,6 @@ const void* batch_kernel_f32(int variant) {
     default: return (const void*)&k_batch_step<float, 1, 16>;
   }
 }
+const void* batch_begin_f32() { return (const void*)&k_batch_begin<float>; }
+const void* batch_fold_f32() { return (const void*)&k_batch_fold<float>; }
 }  // namespace af

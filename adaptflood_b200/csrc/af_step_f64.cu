@@ -22,4 +22,6 @@ const void* batch_kernel_f64(int variant) {
     default: return (const void*)&k_batch_step<double, 1, 16>;
   }
 }
+const void* batch_begin_f64() { return (const void*)&k_batch_begin<double>; }
+const void* batch_fold_f64() { return (const void*)&k_batch_fold<double>; }
 }  // namespace af

@@ -74,9 +74,10 @@ def _fill(cls: int, target_cells: int, cap: int = 256):
 
 def tune_rows(classes: Iterable[int], precision: str = "f32", device: int = 0,
               rows: Sequence[int] = ROWS, target_cells: int = 1 << 25, steps: int = 12,
-              warmup: int = 3, variant: int = -1,
-              arena_bytes: Optional[int] = None) -> Dict[int, int]:
-    """The fastest strip height per size class."""
+              warmup: int = 3, variant: int = -1, arena_bytes: Optional[int] = None,
+              scores_out: Optional[dict] = None) -> Dict[int, int]:
+    """The fastest strip height per size class (`scores_out`, if given,
+    receives the measured cell-updates/s per class and height)."""
     best: Dict[int, int] = {}
     with Batch(precision, device=device, variant=variant, arena_bytes=arena_bytes) as b:
         for cls in classes:
@@ -89,6 +90,8 @@ def tune_rows(classes: Iterable[int], precision: str = "f32", device: int = 0,
                 b.set_rows(cls, r)
                 scores[r] = _rate(b, cases, steps, warmup)
             best[cls] = max(scores, key=scores.get)
+            if scores_out is not None:
+                scores_out[cls] = scores
             b.set_rows(cls, best[cls])
     return best
 

@@ -251,8 +251,8 @@ int af_sim_mass_series(af_sim* s, double* t, double* vol, double* area, int cap,
 typedef struct af_batch af_batch;
 
 /* precision: AF_PREC_F32 or AF_PREC_F64.  variant: launch shape of the batch
- * step kernel (0..4, warps per block x resident blocks per SM), -1 = the
- * default. */
+ * step kernel (0..4: warps per block x resident blocks per SM = 1x16, 1x12,
+ * 1x20, 4x4, 2x8), -1 = the default (1x12). */
 int af_batch_create(int precision, int device, uint64_t arena_bytes, int variant,
                     af_batch** out);
 int af_batch_destroy(af_batch* b);
@@ -288,8 +288,16 @@ int af_batch_attention(af_batch* b);
 int af_batch_query(af_batch* b);
 /* Waits for the launch; AF_ESTATE if the batch's state is invalid. */
 int af_batch_sync(af_batch* b);
-/* af_batch_launch(b, max_steps, 0) + af_batch_sync. */
+/* Steps until every member has finished or max_steps batch steps have run,
+ * and waits.  With the load-adaptive strip height on, it launches once per
+ * scenario completion so the strips are re-cut for the members that remain. */
 int af_batch_run(af_batch* b, int64_t max_steps, int64_t* batch_steps);
+/* Load-adaptive strip height: before each launch, the strip height of every
+ * active member is the tuned height of its size class, lowered (powers of
+ * two, at least 2 rows) until the active members give each warp of the
+ * persistent grid about strips_per_warp strips.  0 turns it off (default 6).
+ * Results do not depend on it. */
+int af_batch_set_balance(af_batch* b, int strips_per_warp);
 
 /* Status of a slot as of the last sync.  *state: 0 running, 1 finished
  * (t >= t_stop), -1 stopped on a bad state (non-finite or non-positive dt). */

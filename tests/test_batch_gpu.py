@@ -87,8 +87,9 @@ def test_strip_height_does_not_change_results(cuda, prec):
     case = _cases()[1]
     cls = size_class(case.nx, case.ny)
     out = []
-    for rows in (1, 3, 8, 64):
+    for rows, balance in ((1, 0), (3, 0), (8, 0), (64, 0), (64, 6)):
         with Batch(prec, arena_bytes=ARENA) as b:
+            b.set_balance(balance)  # 0: fixed strip height; 6: re-cut as load changes
             b.set_rows(cls, rows)
             s = b.add(case)
             b.run()
