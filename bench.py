@@ -1,23 +1,34 @@
 """Throughput benchmark of the local-inertial time step (cell-updates/s).
 
-Workload (the large single plain run): an 8192 x 8192 grid at 5 m with the
-seeded DEM generator, 4096 QVAR triangular hydrographs at wet-prone cells,
-piecewise 0-50 mm/h rain, an HVAR sinusoidal edge depth and FREE edges,
-started at t = 1800 s from a flooded state (a 25 mm film on every cell and the
-channel filled to 2 m) so that every face is wet.  A step is one time step of
-the whole grid: fluxes, edges, sources, rain, depth update, point BCs and the
-Hmax reduction that sets the next dt.
+Headline workload (the large single plain run): an 8192 x 8192 grid at 5 m
+with the seeded DEM generator, 4096 QVAR triangular hydrographs at wet-prone
+cells, piecewise 0-50 mm/h rain, an HVAR sinusoidal edge depth and FREE
+edges, started at t = 1800 s from a flooded state (a 25 mm film on every cell
+and the channel filled to 2 m) so that every face is wet.  A step is one time
+step of the whole grid: fluxes, edges, sources, rain, depth update, point BCs
+and the Hmax reduction that sets the next dt.
 
 Our arm times K steps of the fused kernel (one CUDA-graph launch, CUDA events
 on the simulation's stream) in FP32 (the headline `value`) and FP64, reports
 the HBM roofline of the step kernel, the end-to-end rate through the public
 C ABI with host buffers, and the reference's own CPU code timed on a bounded
-sample of the same workload.  `--impl reference` runs the reference's CPU code
-alone (oracle/_ref, built from the reference sources against the Kokkos-API
-shim), on this host's cores.
+sample of the same workload.  Two more legs (N = 1 only):
 
-N > 1 (torchrun): every rank runs an independent replica of the workload
-(scaling "weak"; the time step needs no data exchange between replicas).
+* `ensemble`: 256 scenarios of 256^2..2048^2 cells, each with its own dt,
+  from t = 0 to 1800 s in one batch (FP32 state, FP64 time and mass), timed
+  as one run; beside it a sample of the same scenarios on the plain FP64
+  single-grid path, one at a time;
+* `serving`: Poisson request streams (grids 128^2..4096^2, sim_time
+  600..3600 s) served by continuous batching at several rates, p50/p99
+  latency from arrival to the depth field on the host, and the same stream
+  served one request at a time by the plain FP64 path.
+
+`--impl reference` runs the reference's CPU code alone (oracle/_ref, built
+from the reference sources against the Kokkos-API shim), on this host's cores.
+
+N > 1 (torchrun): every rank runs an independent replica of the headline
+workload (scaling "weak"; the time step needs no data exchange between
+replicas).
 """
 from __future__ import annotations
 
@@ -50,8 +61,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0,
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", choices=["f32", "f64"], default=None,
-                    help="time one precision only (profiling runs)")
+    ap.add_argument("--only", choices=["f32", "f64", "batch"], default=None,
+                    help="profiling runs: one precision of the single-grid step, or the "
+                         "batch step on --batch-copies copies of the --size grid (FP32)")
+    ap.add_argument("--batch-copies", type=int, default=16)
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--ensemble", type=int, default=256,
                     help="scenarios of the batched-ensemble leg (0 = skip)")
@@ -210,6 +223,25 @@ def time_fused(case, forcing, precision, steps, warmup, device, dist=None):
     return ms, {"t_end": t, "dt_last": dt, "hmax": hmax}
 
 
+def time_batch_copies(case, forcing, copies, steps, warmup, device):
+    """K batch steps of `copies` copies of the flooded workload grid (FP32,
+    fixed strip height), CUDA events on the batch's stream."""
+    import torch
+    from adaptflood_b200.batch import Batch
+    with Batch("f32", device=device) as b:
+        b.set_balance(0)
+        for _ in range(copies):
+            b.add(case, forcing, t_stop=1e30)
+        b.run(max_steps=warmup)
+        stream, e0, e1 = _event_timer(b.stream, device)
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        b.launch(max_steps=steps)
+        e1.record(stream)
+        b.sync()
+        return e0.elapsed_time(e1), case.cells * copies
+
+
 def time_e2e(case, forcing, precision, steps, device):
     """The public C ABI end to end with host buffers: af_sim_create from host
     arrays (DEM, start state, forcing: H2D), the K steps, af_sim_get_state
@@ -366,6 +398,14 @@ def run_ours(args, rank: int, world: int):
     case, forcing = workload(args.size)
     peak, peak_kind = measured_peak()
 
+    if args.only == "batch":
+        ms, cells = time_batch_copies(case, forcing, args.batch_copies, args.steps, args.warmup,
+                                      local)
+        if rank == 0:
+            print(json.dumps({"profiling_run": "batch", "copies": args.batch_copies,
+                              "ms_per_step": ms / args.steps,
+                              "cell_updates_per_s": cells * args.steps / (ms / 1e3)}))
+        return
     if args.only is not None:
         ms, info = time_fused(case, forcing, args.only, args.steps, args.warmup, local, dist)
         if rank == 0:
