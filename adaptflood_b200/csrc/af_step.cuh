@@ -146,6 +146,15 @@ __device__ inline T west_free(T h0, T z0, T h1, T z1, T g, T dx, T nodata) {
   }
   return T(0);
 }
+// FP32: the same edge law with the head difference formed from differences
+// of close values (see flux2); y0 > z0 is h0 > 0 there.
+template <>
+__device__ inline float west_free<float>(float h0, float z0, float h1, float z1, float g, float dx,
+                                         float nodata) {
+  if (z0 == nodata || h0 < 0.001f) return 0.0f;
+  if (h0 > 0.0f && (z1 - z0) + (h1 - h0) < 0.0f) return -h0 * sqrtf(g * h0) * dx * 0.5f;
+  return 0.0f;
+}
 template <typename T>
 __device__ inline T out_free(T h0, T z0, T sign, T g, T dx, T nodata) {
   if (z0 == nodata || h0 < T(0.001)) return T(0);
@@ -288,16 +297,23 @@ __device__ inline float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float2 q0, float2 qa,
                                float2 qb, float2 qc, float2 qd, bool enable,
                                const Phys<float>& ph, bool& any) {
-  const float2 y0 = __fadd2_rn(z0, h0), y1 = __fadd2_rn(z1, h1);
-  const float2 hfx = f2(fmaxf(y0.x, y1.x) - fmaxf(z0.x, z1.x),
-                        fmaxf(y0.y, y1.y) - fmaxf(z0.y, z1.y));
+  // Water-surface elevations y = z + h are never formed: in FP32 their ulp
+  // (2-8 um at 16-64 m of elevation) would give a lake at rest spurious
+  // surface gradients that drive oscillations in deep, weakly damped water.
+  // The head difference y0 - y1 = (z0 - z1) + (h0 - h1) and the flow depth
+  // max(y0,y1) - max(z0,z1) = h_up + min(0, z_up - z_down) are the same
+  // quantities from differences of close values (exact or nearly so).
+  const float2 dz = __fadd2_rn(z0, f2(-z1.x, -z1.y));
+  const float2 dh = __fadd2_rn(dz, __fadd2_rn(h0, f2(-h1.x, -h1.y)));
+  const float2 hfx = f2(dh.x >= 0.0f ? h0.x + fminf(0.0f, dz.x) : h1.x + fminf(0.0f, -dz.x),
+                        dh.y >= 0.0f ? h0.y + fminf(0.0f, dz.y) : h1.y + fminf(0.0f, -dz.y));
   const float2 hf = f2(fminf(fmaxf(hfx.x, 0.0f), ph.max_hflow),
                        fminf(fmaxf(hfx.y, 0.0f), ph.max_hflow));
   const bool wx = enable && z0.x != ph.nodata && z1.x != ph.nodata && hf.x > ph.depth_thresh;
   const bool wy = enable && z0.y != ph.nodata && z1.y != ph.nodata && hf.y > ph.depth_thresh;
   any |= wx | wy;
-  // dh/dx = (y0 - y1)/dx; numerator = q0 - g*dt*hflow*Sf = q0 + g*dt*hflow*dh/dx
-  const float2 s = __fmul2_rn(__ffma2_rn(y1, f2(-1.0f, -1.0f), y0), f2(ph.dxinv, ph.dxinv));
+  // numerator = q0 - g*dt*hflow*Sf = q0 + g*dt*hflow*dh/dx
+  const float2 s = __fmul2_rn(dh, f2(ph.dxinv, ph.dxinv));
   const float2 a = __fmul2_rn(f2(ph.gdt, ph.gdt), hf);
   const float2 num = __ffma2_rn(a, s, q0);
   const float2 qavg = __fmul2_rn(__fadd2_rn(__fadd2_rn(qa, qb), __fadd2_rn(qc, qd)),
@@ -427,7 +443,12 @@ struct BoolC {
 
 // Depth update of a lane's cells: rain (src/kernels.cpp:360-365) then the
 // flux divergence (src/kernels.cpp:286-287).  FP64 keeps the reference's
-// expression; FP32 uses packed FP32x2 with dt/dA folded into one factor.
+// expressions and order.  FP32 forms the cell's whole increment first,
+// rain + (dt/dA)*(flux divergence) (one packed FMA), and rounds it into the
+// depth once: adding the same small rain increment to every depth on its own
+// would round it the same way in every cell of a binade (a bias in the
+// volume), while the flux term differs from cell to cell.  The reference's
+// clamp between rain and update has no effect there (rain >= 0, depth >= 0).
 __device__ inline void update_cells(double (&hn)[2], const double (&qw)[2], const double (&qe)[2],
                                     const double (&qn)[2], const double (&qs)[2],
                                     const double (&z)[2], bool rain_on, double rain_depth,
@@ -448,16 +469,15 @@ __device__ inline void update_cells(float (&hn)[4], const float (&qw)[4], const 
                                     const float (&qn)[4], const float (&qs)[4],
                                     const float (&z)[4], bool rain_on, float rain_depth,
                                     float /*dt*/, float /*dA*/, float dt_dA, float nodata) {
-  if (rain_on) {
+  float rk[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++)
-      if (z[k] != nodata) hn[k] = fmaxf(hn[k] + rain_depth, 0.0f);
-  }
+  for (int k = 0; k < 4; k++) rk[k] = (rain_on && z[k] != nodata) ? rain_depth : 0.0f;
 #pragma unroll
   for (int k = 0; k < 4; k += 2) {
     const float2 a = __ffma2_rn(f2(qe[k], qe[k + 1]), f2(-1.0f, -1.0f), f2(qw[k], qw[k + 1]));
     const float2 b = __ffma2_rn(f2(qs[k], qs[k + 1]), f2(-1.0f, -1.0f), f2(qn[k], qn[k + 1]));
-    const float2 v = __ffma2_rn(f2(dt_dA, dt_dA), __fadd2_rn(a, b), f2(hn[k], hn[k + 1]));
+    const float2 inc = __ffma2_rn(f2(dt_dA, dt_dA), __fadd2_rn(a, b), f2(rk[k], rk[k + 1]));
+    const float2 v = __fadd2_rn(f2(hn[k], hn[k + 1]), inc);
     hn[k] = fmaxf(v.x, 0.0f);
     hn[k + 1] = fmaxf(v.y, 0.0f);
   }

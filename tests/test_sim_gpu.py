@@ -142,7 +142,12 @@ def test_mass_series_matches_reference_reports(cuda):
     assert area_now == float(exp["area"])
 
 
-@pytest.mark.parametrize("name", ["closed_rain_points", "centre_source"])
+# Golden cases in the well-conditioned regime.  closed_rain_points ponds
+# water 0.5 m deep in a 3 m channel of a closed box, where the reference's
+# theta = 1 scheme amplifies any perturbation by about 15 % per step (FP64
+# against FP64 with the DEM moved by 1e-9 m diverges the same way), so an
+# FP32-versus-FP64 comparison there measures that growth, not FP32 error.
+@pytest.mark.parametrize("name", ["centre_source", "east_south_rain"])
 def test_fp32_within_tolerance_of_fp64(cuda, name):
     case, f, exp = load_golden(name)
     with Simulation(case, "f32", forcing=f) as s:
@@ -245,3 +250,26 @@ def test_fused_equals_dropin_kernels_bitwise(cuda, nx, ny, seed, kw):
             np.testing.assert_array_equal(st["H"].ravel(), H.cpu().numpy(), err_msg=f"step {step}")
             np.testing.assert_array_equal(st["Qx"].ravel(), Qx.cpu().numpy())
             np.testing.assert_array_equal(st["Qy"].ravel(), Qy.cpu().numpy())
+
+
+def test_fp32_rain_on_deep_water_conserves_mass(cuda):
+    """Light rain on deep water in a closed box: each step's rain is a few
+    ulps of the FP32 depth, the case where round-to-nearest loses it
+    systematically.  The FP32 volume stays within 1e-6 of the FP64 volume and
+    of the volume the rain adds."""
+    case = sc.small_case(200, 150, seed=41, free=(0, 0, 0, 0), n_qfix=0, n_qvar=0,
+                         sim_time=600.0, channel=False)
+    case.h0 = np.full((case.ny, case.nx), 2.0)
+    case.rain_times = np.array([0.0, 1e4])
+    case.rain_rates = np.array([0.5e-3 / 3600.0] * 2)  # 0.5 mm/h
+    f = fc.pack(case)
+    vols = {}
+    for prec in ("f64", "f32"):
+        with Simulation(case, prec, forcing=f) as s:
+            s.run(case.sim_time)
+            vols[prec], _ = s.volume()
+            t = s.t
+    v0 = 2.0 * case.cells * case.dx ** 2
+    added = 0.5e-3 / 3600.0 * t * case.cells * case.dx ** 2
+    assert abs(vols["f64"] - (v0 + added)) <= 1e-9 * v0
+    assert abs(vols["f32"] - vols["f64"]) <= FP32_MASS_TOL * vols["f64"]
