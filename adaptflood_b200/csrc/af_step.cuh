@@ -131,7 +131,7 @@ template <typename T>
 struct Phys {
   T dx, fn, depth_thresh, max_hflow, nodata, gdt;  // gdt = g*dt
   T g;
-  T dxinv, gdt_fn2;  // 1/dx and g*dt*fn*fn (FP32 form only)
+  T dxinv, gdt_fn2;  // 1/dx and g*dt*fn*fn/dx (FP32 form only)
 };
 
 // FREE edges (src/kernels.cpp:154-248).  West also needs the cell east of
@@ -312,18 +312,18 @@ __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float
   const bool wx = enable && z0.x != ph.nodata && z1.x != ph.nodata && hf.x > ph.depth_thresh;
   const bool wy = enable && z0.y != ph.nodata && z1.y != ph.nodata && hf.y > ph.depth_thresh;
   any |= wx | wy;
-  // numerator = q0 - g*dt*hflow*Sf = q0 + g*dt*hflow*dh/dx
-  const float2 s = __fmul2_rn(dh, f2(ph.dxinv, ph.dxinv));
+  // In units of the stored Q (= Qold*dx): the reference's
+  //   Q = (Qold - g*dt*hflow*Sf) / (1 + g*dt*n^2*|Qvect|/hflow^(10/3)) * dx
+  // with Sf = -dh/dx is Q = (Q0 + g*dt*hflow*dh) / (1 + g*dt*n^2/dx*|Qv|*hflow^(-7/3)).
   const float2 a = __fmul2_rn(f2(ph.gdt, ph.gdt), hf);
-  const float2 num = __ffma2_rn(a, s, q0);
+  const float2 num = __ffma2_rn(a, dh, q0);
   const float2 qavg = __fmul2_rn(__fadd2_rn(__fadd2_rn(qa, qb), __fadd2_rn(qc, qd)),
                                  f2(0.25f, 0.25f));
   const float2 qv2 = __ffma2_rn(q0, q0, __fmul2_rn(qavg, qavg));
   const float2 qv = f2(sqrtf(qv2.x), sqrtf(qv2.y));
   const float2 pw = f2(exp2f(-7.0f / 3.0f * __log2f(hf.x)), exp2f(-7.0f / 3.0f * __log2f(hf.y)));
   const float2 den = __ffma2_rn(__fmul2_rn(f2(ph.gdt_fn2, ph.gdt_fn2), qv), pw, f2(1.0f, 1.0f));
-  const float2 nd = __fmul2_rn(num, f2(ph.dx, ph.dx));
-  return f2(wx ? __fdividef(nd.x, den.x) : 0.0f, wy ? __fdividef(nd.y, den.y) : 0.0f);
+  return f2(wx ? __fdividef(num.x, den.x) : 0.0f, wy ? __fdividef(num.y, den.y) : 0.0f);
 }
 
 __device__ inline void row_faces(const float (&h)[4], const float (&z)[4], const float (&hN)[4],
@@ -522,7 +522,7 @@ __device__ inline void fill_scalars(const StepParams& p, double t, double dt, do
   s.ph.g = T(p.g);
   s.ph.gdt = T(p.g * dt);  // (g*dt) rounded once, as the reference's left-to-right product does
   s.ph.dxinv = T(1.0 / p.dx);
-  s.ph.gdt_fn2 = T(p.g * dt * p.fpn * p.fpn);
+  s.ph.gdt_fn2 = T(p.g * dt * p.fpn * p.fpn * p.dxinv);
 }
 
 template <typename T>
@@ -532,13 +532,14 @@ __device__ inline void step_scalars(const StepParams& p, double t, double hmax_p
 }
 
 // What one lane carries out of its strips: the max depth over its valid
-// cells (state precision; exact) and, at mass-report steps, its volume and
-// flooded-area sums.
+// cells (state precision; exact; -FLT_MAX while it has seen none: depths of
+// valid cells are finite and far above it) and, at mass-report steps, its
+// volume and flooded-area sums.
 template <typename T>
 struct LaneAcc {
   T m_cell;
-  bool any_cell;
   double v, a;
+  __device__ bool any_cell() const { return m_cell != T(-FLT_MAX); }
 };
 
 // One step of strip (sx, sy) of one grid by one warp: the strip's OWN
@@ -554,6 +555,9 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
   constexpr int N = Lanes<T>::N;
   constexpr int OWN = 30 * N;
   static_assert(32 * N * sizeof(T) == kRowBytes, "one 16-byte vector per lane");
+  // FP64 forms the reference's Qold = Q*(1/dx) on load (its exact rounding);
+  // the FP32 face law works on Q itself (1/dx folded into its coefficients).
+  constexpr bool kQold = Lanes<T>::N == 2;
   const int lane = threadIdx.x & 31;
   const int nx = p.nx, ny = p.ny, P = p.P;
   const int parity = sc.parity;
@@ -637,8 +641,10 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
       release();
 #pragma unroll
       for (int k = 0; k < N; k++) {
-        qxo[k] = qxo[k] * dxinvT;
-        qyo[k] = qyo[k] * dxinvT;
+        if (kQold) {
+          qxo[k] = qxo[k] * dxinvT;
+          qyo[k] = qyo[k] * dxinvT;
+        }
       }
     }
   }
@@ -662,7 +668,8 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
       // same flux through their common edge, bit for bit, in either
       // precision.  The west faces it also returns are not needed here.
 #pragma unroll
-      for (int k = 0; k < N; k++) qxp[k] = qxp[k] * dxinvT;
+      for (int k = 0; k < N; k++)
+        if (kQold) qxp[k] = qxp[k] * dxinvT;
       const T qxpR = __shfl_down_sync(0xffffffffu, qxp[0], 1);
       const T qxoR = __shfl_down_sync(0xffffffffu, qxo[0], 1);
       T qw_unused[N];
@@ -695,8 +702,10 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
         release();
 #pragma unroll
         for (int k = 0; k < N; k++) {
-          qyoN[k] = qyoN[k] * dxinvT;
-          qxoN[k] = qxoN[k] * dxinvT;
+          if (kQold) {
+            qyoN[k] = qyoN[k] * dxinvT;
+            qxoN[k] = qxoN[k] * dxinvT;
+          }
         }
       }
       // Neighbours across lanes.
@@ -789,14 +798,15 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
           }
         }
         if (kEdge && cb <= nx - 1 && nx - 1 < cb + N) Qxn[(long long)j * P + nx] = qe_last;
+        // Hmax over valid cells (a NaN never wins the comparison).
 #pragma unroll
-        for (int k = 0; k < N; k++) {
-          if (!kEdge || cb + k < nx) {
-            if (z[k] != ph.nodata) {
-              acc.any_cell = true;
-              if (hn[k] > acc.m_cell) acc.m_cell = hn[k];
-            }
-            if (mass) {
+        for (int k = 0; k < N; k++)
+          if ((!kEdge || cb + k < nx) && z[k] != ph.nodata)
+            acc.m_cell = (hn[k] > acc.m_cell) ? hn[k] : acc.m_cell;
+        if (__builtin_expect(mass, 0)) {  // warp-uniform: mass-report steps only
+#pragma unroll
+          for (int k = 0; k < N; k++) {
+            if (!kEdge || cb + k < nx) {
               const double hv = (double)hn[k];
               acc.v += hv * p.dA;
               if (hv > 0.01) acc.a += p.dA;
@@ -898,7 +908,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
   }
   __syncwarp();
   int kglob = 0;
-  LaneAcc<T> acc{T(-FLT_MAX), false, 0.0, 0.0};
+  LaneAcc<T> acc{T(-FLT_MAX), 0.0, 0.0};
   const int tiles_y = (p.nsy + WY - 1) / WY;
   const int ntiles = p.nsx * tiles_y;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -911,7 +921,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
   // A valid cell's depth is finite (NaN never wins a comparison), and in
   // FP64 m_cell is exact; a lane with no valid cell keeps the identity.
   double m_loc = -DBL_MAX, v_loc = acc.v, a_loc = acc.a;
-  if (acc.any_cell && (double)acc.m_cell > m_loc) m_loc = (double)acc.m_cell;
+  if (acc.any_cell() && (double)acc.m_cell > m_loc) m_loc = (double)acc.m_cell;
 
   // ----- block reductions: Hmax, and volume/area at mass-report steps -----
   __shared__ double s_m[WY], s_v[WY], s_a[WY];
@@ -1228,9 +1238,9 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams 
       __syncwarp();
     }
     const int k = u - tab->u0[a];
-    LaneAcc<T> acc{T(-FLT_MAX), false, 0.0, 0.0};
+    LaneAcc<T> acc{T(-FLT_MAX), 0.0, 0.0};
     const bool ok = run_strip<T>(p, sc, k % p.nsx, k / p.nsx, s_ring[warp], bar, kglob, acc);
-    double m = (acc.any_cell) ? (double)acc.m_cell : -DBL_MAX;
+    double m = acc.any_cell() ? (double)acc.m_cell : -DBL_MAX;
     m = warp_maxd(m);
     double v = 0.0, ar = 0.0;
     if (sc.mass) {
