@@ -39,6 +39,15 @@ class CaseDesc(C.Structure):
     ]
 
 
+class OutputDesc(C.Structure):
+    _fields_ = [
+        ("out_dir", C.c_char_p), ("save_int", C.c_double), ("voutput", C.c_int),
+        ("async_style", C.c_int), ("xll", C.c_double), ("yll", C.c_double),
+        ("n_stage", C.c_int), ("stage_idx", C.c_void_p), ("stage_names", C.c_void_p),
+        ("stage_int", C.c_double),
+    ]
+
+
 class ForcingDesc(C.Structure):
     _fields_ = [
         ("n_flow", C.c_int), ("flow_idx", C.c_void_p), ("flow_type", C.c_void_p),
@@ -83,6 +92,8 @@ _SIGS = {
     "af_sim_velocity": (_i, [_vp, _vp, _vp]),
     "af_sim_volume": (_i, [_vp, _vp, _vp]),
     "af_sim_mass_series": (_i, [_vp, _vp, _vp, _vp, _i, _vp]),
+    "af_sim_run_output": (_i, [_vp, _d, _vp, _vp]),
+    "af_write_asc": (_i, [C.c_char_p, _vp, _i, _i, _d, _d, _d, _d, _i]),
     "af_batch_create": (_i, [_i, _i, _u64, _i, _vp]),
     "af_batch_destroy": (_i, [_vp]),
     "af_batch_size_class": (_i, [_i, _i]),

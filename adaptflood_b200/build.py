@@ -37,8 +37,8 @@ UNITS = [
     ("af_sim.cu", EXACT),
     ("af_batch.cu", EXACT),
 ]
-HOST_UNITS = ["af_io.cpp", "af_arena.cpp"]
-HEADERS = ["af_common.cuh", "af_step.cuh", "af_simcore.cuh", "af_arena.h"]
+HOST_UNITS = ["af_io.cpp", "af_arena.cpp", "af_output.cpp"]
+HEADERS = ["af_common.cuh", "af_step.cuh", "af_simcore.cuh", "af_arena.h", "af_output.h"]
 
 
 def _newer(target: str, deps) -> bool:
@@ -78,7 +78,7 @@ def build(verbose: bool = False, ptxas_info: bool = False, obj_dir: str = None, 
         o = os.path.join(OBJ, src + ".o")
         objs.append(o)
         if _newer(o, [s, __file__] + hdrs):
-            jobs.append([HOSTCXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off",
+            jobs.append([HOSTCXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread",
                          "-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o])
     log = []
     with cf.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:

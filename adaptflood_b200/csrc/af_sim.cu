@@ -6,6 +6,7 @@
 // launch: a begin kernel sets the stop condition, then a conditional WHILE
 // node re-runs the step kernel until its last block clears the condition.
 #include <algorithm>
+#include <cerrno>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -13,6 +14,9 @@
 #include <numeric>
 #include <vector>
 
+#include <sys/stat.h>
+
+#include "af_output.h"
 #include "af_simcore.cuh"
 
 namespace af {
@@ -174,6 +178,51 @@ __global__ void k_begin(SimCtl* ctl, double t_stop, long long max_steps,
   ctl->done = done;
   ctl->arrive = 0u;
   if (use_cond) cudaGraphSetConditional(cond, done ? 0u : 1u);
+}
+
+// Snapshot of the state for the file outputs: H and, when asked, the
+// velocity of ComputeVelocity_GPU (src/kernels.cpp:293-351), as dense FP64
+// fields in the reference layout.
+template <typename T>
+__global__ void k_snapshot(const T* __restrict__ H, const T* __restrict__ Z,
+                           const T* __restrict__ Qx, const T* __restrict__ Qy, int nx, int ny,
+                           int P, double dx, double nodata, double* __restrict__ oH,
+                           double* __restrict__ oVx, double* __restrict__ oVy) {
+  const long long n = (long long)nx * ny;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(k / nx), i = (int)(k - (long long)j * nx);
+    const long long r = (long long)j * P;
+    const double h = (double)H[r + i];
+    oH[k] = h;
+    if (!oVx) continue;
+    const double z = (double)Z[r + i];
+    if (z == (double)T(nodata) || h < 0.001) {
+      oVx[k] = 0.0;
+      oVy[k] = 0.0;
+      continue;
+    }
+    double hflow = h;
+    if (hflow < 0.001) hflow = 0.001;
+    const double ql = (double)Qx[r + i], qr = (double)Qx[r + i + 1];
+    const double vl = (fabs(ql) > 1e-10) ? ql / dx / hflow : 0.0;
+    const double vr = (fabs(qr) > 1e-10) ? qr / dx / hflow : 0.0;
+    oVx[k] = (fabs(vl) > fabs(vr)) ? vl : vr;
+    const double qt = (double)Qy[r + i], qb = (double)Qy[r + P + i];
+    const double vt = (fabs(qt) > 1e-10) ? qt / dx / hflow : 0.0;
+    const double vb = (fabs(qb) > 1e-10) ? qb / dx / hflow : 0.0;
+    oVy[k] = (fabs(vt) > fabs(vb)) ? vt : vb;
+  }
+}
+
+// Depths at the stage points (src/main.cpp:306-322); -1 = outside the grid.
+template <typename T>
+__global__ void k_gather(const T* __restrict__ H, int nx, int P, const int* __restrict__ idx,
+                         int n, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int c = idx[k];
+  out[k] = c < 0 ? 0.0 : (double)H[(long long)(c / nx) * P + c % nx];
 }
 
 // ----------------------------------------------------------- the object
@@ -726,6 +775,207 @@ int af_sim_mass_series(af_sim* h, double* t, double* vol, double* area, int cap,
   }
   *n = s.pinned_ctl->mass_count;
   return AF_OK;
+}
+
+}  // extern "C"
+
+namespace af {
+
+// The reference's main loop with its file outputs (src/main.cpp:196-388): the
+// state at t = 0 as H_0000.asc, one save each time a step ends at or past the
+// next save time, stage-point depths each time a step ends at or past the next
+// stage time, and H_final.asc (+ Vx/Vy_final.asc) at the end.  The GPU keeps
+// stepping while a save is copied out (copy stream) and written (writer
+// thread): the snapshot kernel copies the state into a device buffer first.
+static int run_output(Sim& s, double sim_time, const af_output_desc& o, int64_t* steps_out) {
+  AF_CUDA(cudaSetDevice(s.device));
+  if (!o.out_dir) return AF_EINVAL;
+  if (::mkdir(o.out_dir, 0755) != 0 && errno != EEXIST) return AF_EIO;  // src/main.cpp:130
+  const int nx = s.c.nx, ny = s.c.ny;
+  const size_t cells = (size_t)nx * ny;
+  const bool vel = o.voutput != 0;
+  const int nf = vel ? 3 : 1;
+  const int style = o.async_style ? kAscAsync : kAscSync;
+  const std::string dir(o.out_dir);
+  DevBuf dsnap, didx, dval;
+  AF_TRY(alloc_field(dsnap, cells * nf, 8));
+  std::unique_ptr<double, decltype(&cudaFreeHost)> hsnap(nullptr, &cudaFreeHost);
+  std::unique_ptr<double, decltype(&cudaFreeHost)> hval(nullptr, &cudaFreeHost);
+  {
+    double* p = nullptr;
+    AF_CUDA(cudaMallocHost((void**)&p, cells * nf * sizeof(double)));
+    hsnap.reset(p);
+  }
+  struct Streams {
+    cudaStream_t cst = nullptr;
+    cudaEvent_t ev_snap = nullptr, ev_copy = nullptr;
+    ~Streams() {
+      if (cst) cudaStreamSynchronize(cst);
+      if (ev_snap) cudaEventDestroy(ev_snap);
+      if (ev_copy) cudaEventDestroy(ev_copy);
+      if (cst) cudaStreamDestroy(cst);
+    }
+  } R;
+  AF_CUDA(cudaStreamCreateWithFlags(&R.cst, cudaStreamNonBlocking));
+  AF_CUDA(cudaEventCreateWithFlags(&R.ev_snap, cudaEventDisableTiming));
+  AF_CUDA(cudaEventCreateWithFlags(&R.ev_copy, cudaEventDisableTiming));
+  AF_CUDA(cudaEventRecord(R.ev_copy, R.cst));
+  const int nst = std::max(0, o.n_stage);
+  FILE* stage_fp = nullptr;
+  if (nst > 0) {
+    std::vector<int> idx(o.stage_idx, o.stage_idx + nst);
+    for (int& c : idx)
+      if (c < 0 || (size_t)c >= cells) c = -1;
+    AF_TRY(upload(didx, idx, s.st));
+    AF_TRY(alloc_field(dval, nst, 8));
+    double* p = nullptr;
+    AF_CUDA(cudaMallocHost((void**)&p, nst * sizeof(double)));
+    hval.reset(p);
+    stage_fp = fopen((dir + "/stage.csv").c_str(), "w");  // src/main.cpp:100-108
+    if (!stage_fp) return AF_EIO;
+    fprintf(stage_fp, "Time(s)");
+    for (int k = 0; k < nst; k++) {
+      if (o.stage_names && o.stage_names[k]) fprintf(stage_fp, ",%s", o.stage_names[k]);
+      else fprintf(stage_fp, ",Stage%d", k + 1);
+    }
+    fprintf(stage_fp, "\n");
+  }
+  std::unique_ptr<FILE, int (*)(FILE*)> stage_guard(stage_fp, [](FILE* f) {
+    return f ? fclose(f) : 0;
+  });
+  Writer writer;
+  double* snap = static_cast<double*>(dsnap.p);
+
+  // A save is two halves.  snapshot(): the state into the device buffer
+  // (after the previous save's copy has left it), on the simulation stream,
+  // before the next segment changes the state.  ship(): issued once the next
+  // segment is queued, so the GPU keeps stepping meanwhile: the copy to pinned
+  // host memory on the copy stream (after the writer has finished with it)
+  // and the files on the writer thread.
+  struct Pending {
+    bool on = false;
+    std::string tag;
+    int style = 0;
+    bool velocity = false;
+  } pend;
+  auto snapshot = [&](const std::string& tag, int st, bool velocity) -> int {
+    AF_TRY(read_ctl(s));
+    const int par = s.pinned_ctl->parity;
+    AF_CUDA(cudaStreamWaitEvent(s.st, R.ev_copy, 0));
+    const unsigned g = grid_for((long long)cells, 256, 8);
+    double* vx = velocity ? snap + cells : nullptr;
+    double* vy = velocity ? snap + 2 * cells : nullptr;
+    if (s.prec == AF_PREC_F64)
+      k_snapshot<double><<<g, 256, 0, s.st>>>(
+          s.buf<double>(s.H[par]), s.buf<double>(s.DEM), s.buf<double>(s.Qx[par]),
+          s.buf<double>(s.Qy[par]), nx, ny, s.P, s.c.dx, s.c.nodata, snap, vx, vy);
+    else
+      k_snapshot<float><<<g, 256, 0, s.st>>>(
+          s.buf<float>(s.H[par]), s.buf<float>(s.DEM), s.buf<float>(s.Qx[par]),
+          s.buf<float>(s.Qy[par]), nx, ny, s.P, s.c.dx, s.c.nodata, snap, vx, vy);
+    AF_CUDA(cudaGetLastError());
+    AF_CUDA(cudaEventRecord(R.ev_snap, s.st));
+    pend.on = true;
+    pend.tag = tag;
+    pend.style = st;
+    pend.velocity = velocity;
+    return AF_OK;
+  };
+  auto ship = [&]() -> int {
+    if (!pend.on) return AF_OK;
+    pend.on = false;
+    writer.drain();  // the pinned copy is free again
+    const bool velocity = pend.velocity;
+    const size_t nb = cells * (velocity ? 3 : 1) * sizeof(double);
+    AF_CUDA(cudaStreamWaitEvent(R.cst, R.ev_snap, 0));
+    AF_CUDA(cudaMemcpyAsync(hsnap.get(), snap, nb, cudaMemcpyDeviceToHost, R.cst));
+    AF_CUDA(cudaEventRecord(R.ev_copy, R.cst));
+    const double* h = hsnap.get();
+    const double xll = o.xll, yll = o.yll, cs = s.c.dx, nd = s.c.nodata;
+    const std::string tag = pend.tag;
+    const int st = pend.style;
+    cudaEvent_t ev = R.ev_copy;
+    writer.post([&writer, h, cells, dir, tag, st, velocity, nx, ny, xll, yll, cs, nd, ev] {
+      if (cudaEventSynchronize(ev) != cudaSuccess) {
+        writer.fail();
+        return;
+      }
+      const char* names[3] = {"H", "Vx", "Vy"};
+      for (int f = 0; f < (velocity ? 3 : 1); f++) {
+        const std::string path = dir + "/" + names[f] + "_" + tag + ".asc";
+        if (!write_asc(path.c_str(), h + f * cells, nx, ny, xll, yll, cs, nd, st, 0))
+          writer.fail();
+      }
+    });
+    return AF_OK;
+  };
+  auto tag_of = [](int n) {
+    char b[16];
+    snprintf(b, sizeof b, "%04d", n);
+    return std::string(b);
+  };
+
+  AF_TRY(read_ctl(s));
+  const long long step0 = s.pinned_ctl->step;
+  double t = s.pinned_ctl->t;
+  int save_num = 0;
+  AF_TRY(snapshot(tag_of(save_num++), style, vel && style == kAscAsync));  // src/main.cpp:206-225
+  const double inf = 1e300;
+  double next_save = o.save_int > 0.0 ? o.save_int : inf;  // src/main.cpp:199-201
+  double next_stage = (nst > 0 && o.stage_int > 0.0) ? o.stage_int : inf;
+  while (t < sim_time) {  // src/main.cpp:227
+    const double stop = std::min(sim_time, std::min(next_save, next_stage));
+    // At least one step: a save or stage time already passed is taken after
+    // the next step, one per step, as the reference's loop does.
+    if (t < stop) AF_TRY(launch(s, stop, 0x3FFFFFFFFFFFFFFFLL));
+    else AF_TRY(launch(s, sim_time, 1));
+    AF_TRY(ship());  // the previous save leaves while this segment runs
+    AF_CUDA(cudaStreamSynchronize(s.st));
+    AF_TRY(read_ctl(s));
+    if (s.pinned_ctl->status) return AF_ESTATE;
+    t = s.pinned_ctl->t;
+    if (nst > 0 && t >= next_stage) {  // src/main.cpp:306-322
+      const int par = s.pinned_ctl->parity;
+      if (s.prec == AF_PREC_F64)
+        k_gather<double><<<(nst + 127) / 128, 128, 0, s.st>>>(
+            s.buf<double>(s.H[par]), nx, s.P, (const int*)didx.p, nst, (double*)dval.p);
+      else
+        k_gather<float><<<(nst + 127) / 128, 128, 0, s.st>>>(
+            s.buf<float>(s.H[par]), nx, s.P, (const int*)didx.p, nst, (double*)dval.p);
+      AF_CUDA(cudaMemcpyAsync(hval.get(), dval.p, nst * sizeof(double), cudaMemcpyDeviceToHost,
+                              s.st));
+      AF_CUDA(cudaStreamSynchronize(s.st));
+      fprintf(stage_fp, "%.1f", t);
+      for (int k = 0; k < nst; k++) {
+        const int c = o.stage_idx[k];
+        if (c >= 0 && (size_t)c < cells) fprintf(stage_fp, ",%.4f", hval.get()[k]);
+        else fprintf(stage_fp, ",NaN");
+      }
+      fprintf(stage_fp, "\n");
+      fflush(stage_fp);
+      next_stage += o.stage_int;
+    }
+    if (t >= next_save) {  // src/main.cpp:325-363
+      AF_TRY(snapshot(tag_of(save_num++), style, vel && style == kAscAsync));
+      next_save += o.save_int;
+    }
+  }
+  AF_TRY(ship());
+  // Final state (src/main.cpp:376-388): always the synchronous writer's format.
+  AF_TRY(snapshot("final", kAscSync, vel));
+  AF_TRY(ship());
+  writer.drain();
+  if (steps_out) *steps_out = s.pinned_ctl->step - step0;
+  return writer.errors() ? AF_EIO : AF_OK;
+}
+
+}  // namespace af
+
+extern "C" {
+
+int af_sim_run_output(af_sim* h, double sim_time, const af_output_desc* o, int64_t* steps) {
+  if (!h || !o) return AF_EINVAL;
+  return af::run_output(*h->s, sim_time, *o, steps);
 }
 
 }  // extern "C"

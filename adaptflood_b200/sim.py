@@ -10,6 +10,7 @@ reference's layout; ``velocity()`` is ComputeVelocity_GPU
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import Optional, Tuple
 
 import numpy as np
@@ -156,6 +157,34 @@ class Simulation:
         v, a = C.c_double(), C.c_double()
         _lib.check(self.lib.af_sim_volume(self.h, C.byref(v), C.byref(a)), "af_sim_volume")
         return v.value, a.value
+
+    def run_output(self, out_dir: str, sim_time: Optional[float] = None,
+                   save_int: Optional[float] = None, voutput: bool = False,
+                   async_style: bool = False, stages=None, stage_int: float = 60.0) -> int:
+        """Runs to ``sim_time`` writing the reference's files into ``out_dir``
+        (af_sim_run_output): H_%04d.asc every ``save_int``, H_final.asc, with
+        ``voutput`` the velocity grids, and ``stage.csv`` for ``stages`` (a list
+        of (name, i, j) cells).  Returns the steps taken."""
+        case = self.case
+        o = _lib.OutputDesc()
+        o.out_dir = os.fsencode(out_dir)
+        o.save_int = float(case.save_int if save_int is None else save_int)
+        o.voutput, o.async_style = int(voutput), int(async_style)
+        o.xll, o.yll = case.xll, case.yll
+        keep = []
+        if stages:
+            idx = np.array([j * case.nx + i if 0 <= i < case.nx and 0 <= j < case.ny else -1
+                            for _, i, j in stages], dtype=np.int32)
+            names = (C.c_char_p * len(stages))(*[n.encode() for n, _, _ in stages])
+            keep += [idx, names]
+            o.n_stage, o.stage_idx, o.stage_names = len(stages), idx.ctypes.data, C.addressof(names)
+            o.stage_int = float(stage_int)
+        n = C.c_int64()
+        t_end = case.sim_time if sim_time is None else sim_time
+        _lib.check(self.lib.af_sim_run_output(self.h, float(t_end), C.byref(o), C.byref(n)),
+                   "af_sim_run_output")
+        del keep
+        return n.value
 
     def mass_series(self):
         n = C.c_int()

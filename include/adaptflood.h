@@ -223,6 +223,39 @@ int af_sim_volume(af_sim* s, double* vol, double* area);
  * (src/main.cpp:291-304): up to cap entries of (t, vol, area). */
 int af_sim_mass_series(af_sim* s, double* t, double* vol, double* area, int cap, int* n);
 
+/* Output of a run as the reference's main loop writes it (src/main.cpp:196-388,
+ * src/io.cpp:314-334, src/async_output.cpp:84-176): ESRI ASCII grids with
+ * "%.4f " values in out_dir (created if missing): H_0000.asc for the state at
+ * the start, H_%04d.asc after the first step ending at or past each multiple
+ * of save_int (with Vx_/Vy_%04d.asc too when voutput and async_style, as the
+ * reference's async writer does), stage.csv rows ("%.1f" time, ",%.4f" depth or
+ * ",NaN" off the grid) after the first step ending at or past each multiple of
+ * stage_int, and H_final.asc (+ Vx_/Vy_final.asc with voutput) at the end.
+ * async_style selects the header of the reference's async writer (xll/yll
+ * "%.6f", NODATA "%.0f") rather than its synchronous one ("%.1f", "-9999").
+ * Values are formatted exactly as printf("%.4f") does.  The GPU keeps stepping
+ * while a save is copied out and written by a background thread. */
+typedef struct af_output_desc {
+  const char* out_dir;   /* dirroot                                            */
+  double save_int;       /* saveint; <= 0: no periodic saves                  */
+  int voutput;           /* par key voutput                                   */
+  int async_style;       /* par key async_output                              */
+  double xll, yll;       /* georeference written to the ASC headers           */
+  int n_stage;           /* stage points: cell index (-1: off the grid)       */
+  const int* stage_idx;
+  const char* const* stage_names;  /* NULL entries: "Stage<k>"                */
+  double stage_int;      /* par key stageint                                  */
+} af_output_desc;
+
+/* Runs to sim_time with the outputs above; *steps (optional) = steps taken. */
+int af_sim_run_output(af_sim* s, double sim_time, const af_output_desc* o, int64_t* steps);
+
+/* One ESRI ASCII grid as the reference writes it (row 0 north, values
+ * "%.4f " per cell); style 0 = src/io.cpp:314-334's header, 1 = the async
+ * writer's (src/async_output.cpp:158-167). */
+int af_write_asc(const char* path, const double* values, int ncols, int nrows, double xll,
+                 double yll, double cellsize, double nodata, int style);
+
 /* ======================================================= 3. batch layer == */
 
 /* No counterpart in the reference, which runs one grid per process: a batch
