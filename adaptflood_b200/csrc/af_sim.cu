@@ -309,6 +309,32 @@ static int alloc_field(DevBuf& b, size_t elems, int esize) {
 
 // Copies a host FP64 field with `rows` x `width` entries and host pitch
 // `hpitch` into the padded device field (converted to the sim precision).
+// Field transfers between the caller's FP64 host arrays (rows of `width`
+// values at host pitch `hpitch`) and a padded device field.  FP64 fields are
+// one 2-D copy.  FP32 fields go through a dense FP64 device staging buffer in
+// chunks of rows, converted by a kernel on the device, so the host does no
+// per-element work (and pinned host arrays move at full link bandwidth).
+__global__ void k_pad_from_f64(const double* __restrict__ src, int rows, int width,
+                               float* __restrict__ dst, int P) {
+  const long long n = (long long)rows * width;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const long long j = k / width, i = k - j * width;
+    dst[j * P + i] = (float)src[k];
+  }
+}
+__global__ void k_dense_to_f64(const float* __restrict__ src, int P, int rows, int width,
+                               double* __restrict__ dst) {
+  const long long n = (long long)rows * width;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const long long j = k / width, i = k - j * width;
+    dst[k] = (double)src[j * P + i];
+  }
+}
+
+constexpr size_t kStageBytes = 64u << 20;
+
 static int put_field(Sim& s, DevBuf& b, const double* src, int rows, int width, size_t hpitch) {
   char* dst = static_cast<char*>(b.p) + (size_t)kGuard * s.esize;
   if (s.prec == AF_PREC_F64) {
@@ -317,11 +343,18 @@ static int put_field(Sim& s, DevBuf& b, const double* src, int rows, int width, 
     AF_CUDA(cudaStreamSynchronize(s.st));
     return AF_OK;
   }
-  std::vector<float> tmp((size_t)rows * width);
-  for (int j = 0; j < rows; j++)
-    for (int i = 0; i < width; i++) tmp[(size_t)j * width + i] = (float)src[(size_t)j * hpitch + i];
-  AF_CUDA(cudaMemcpy2DAsync(dst, (size_t)s.P * 4, tmp.data(), (size_t)width * 4,
-                            (size_t)width * 4, rows, cudaMemcpyHostToDevice, s.st));
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>(rows, kStageBytes / (8 * (size_t)width)));
+  DevBuf stage;
+  AF_TRY(alloc_field(stage, (size_t)chunk * width, 8));
+  for (int j = 0; j < rows; j += chunk) {
+    const int n = std::min(chunk, rows - j);
+    AF_CUDA(cudaMemcpy2DAsync(stage.p, (size_t)width * 8, src + (size_t)j * hpitch, hpitch * 8,
+                              (size_t)width * 8, n, cudaMemcpyHostToDevice, s.st));
+    k_pad_from_f64<<<grid_for((long long)n * width, 256, 8), 256, 0, s.st>>>(
+        static_cast<const double*>(stage.p), n, width,
+        reinterpret_cast<float*>(dst) + (size_t)j * s.P, s.P);
+    AF_CUDA(cudaGetLastError());
+  }
   AF_CUDA(cudaStreamSynchronize(s.st));
   return AF_OK;
 }
@@ -334,12 +367,19 @@ static int get_field(Sim& s, DevBuf& b, double* dst, int rows, int width, size_t
     AF_CUDA(cudaStreamSynchronize(s.st));
     return AF_OK;
   }
-  std::vector<float> tmp((size_t)rows * width);
-  AF_CUDA(cudaMemcpy2DAsync(tmp.data(), (size_t)width * 4, src, (size_t)s.P * 4,
-                            (size_t)width * 4, rows, cudaMemcpyDeviceToHost, s.st));
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>(rows, kStageBytes / (8 * (size_t)width)));
+  DevBuf stage;
+  AF_TRY(alloc_field(stage, (size_t)chunk * width, 8));
+  for (int j = 0; j < rows; j += chunk) {
+    const int n = std::min(chunk, rows - j);
+    k_dense_to_f64<<<grid_for((long long)n * width, 256, 8), 256, 0, s.st>>>(
+        reinterpret_cast<const float*>(src) + (size_t)j * s.P, s.P, n, width,
+        static_cast<double*>(stage.p));
+    AF_CUDA(cudaGetLastError());
+    AF_CUDA(cudaMemcpy2DAsync(dst + (size_t)j * hpitch, hpitch * 8, stage.p, (size_t)width * 8,
+                              (size_t)width * 8, n, cudaMemcpyDeviceToHost, s.st));
+  }
   AF_CUDA(cudaStreamSynchronize(s.st));
-  for (int j = 0; j < rows; j++)
-    for (int i = 0; i < width; i++) dst[(size_t)j * hpitch + i] = (double)tmp[(size_t)j * width + i];
   return AF_OK;
 }
 

@@ -123,11 +123,17 @@ class Simulation:
         return self.status()[3]
 
     # ---------------------------------------------------------------- state
-    def state(self, velocity: bool = False) -> dict:
+    def state(self, velocity: bool = False, out: Optional[dict] = None) -> dict:
+        """H, Qx, Qy (FP64, reference layout); `out` may supply the arrays
+        (e.g. in pinned host memory) as {"H", "Qx", "Qy"} of the right sizes."""
         nx, ny = self.nx, self.ny
-        H = np.zeros(nx * ny)
-        Qx = np.zeros((nx + 1) * (ny + 1))
-        Qy = np.zeros((nx + 1) * (ny + 1))
+        if out is not None:
+            H, Qx, Qy = (np.ascontiguousarray(out[k]).reshape(-1) for k in ("H", "Qx", "Qy"))
+            assert H.size == nx * ny and Qx.size == Qy.size == (nx + 1) * (ny + 1)
+        else:
+            H = np.zeros(nx * ny)
+            Qx = np.zeros((nx + 1) * (ny + 1))
+            Qy = np.zeros((nx + 1) * (ny + 1))
         _lib.check(self.lib.af_sim_get_state(self.h, _p(H), _p(Qx), _p(Qy)), "af_sim_get_state")
         out = {"H": H.reshape(ny, nx), "Qx": Qx.reshape(ny + 1, nx + 1),
                "Qy": Qy.reshape(ny + 1, nx + 1)}
