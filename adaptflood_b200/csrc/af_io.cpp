@@ -24,6 +24,7 @@
 // grid, a truncated DEM, or an unreadable .bdy count/value line is an error
 // (AF_ERANGE / AF_EIO) instead of an out-of-bounds index or an uninitialised
 // value; lines are not limited to 255 characters.
+#include <algorithm>
 #include <cerrno>
 #include <cstdio>
 #include <cstdlib>
@@ -31,6 +32,7 @@
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "adaptflood.h"
@@ -110,28 +112,70 @@ int read_par(const char* path, Par& p) {
   return AF_OK;
 }
 
-// src/io.cpp:132-161, with a whole-file buffer and strtod (the same
-// correctly rounded conversion fscanf("%lf") performs).
+static inline bool is_ws(char c) {
+  return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\v' || c == '\f';
+}
+
+// Parses the whitespace-separated values of [s, end) into out (at most cap
+// values); each token is converted by strtod and must be consumed entirely.
+// Returns the number of tokens, or -1 on a malformed token.
+static long long parse_values(const char* s, const char* end, double* out, long long cap) {
+  long long n = 0;
+  while (s < end) {
+    while (s < end && is_ws(*s)) s++;
+    if (s >= end) break;
+    const char* t = s;
+    while (t < end && !is_ws(*t)) t++;
+    if (n < cap) {
+      char* e = nullptr;
+      out[n] = strtod(s, &e);
+      if (e != t) return -1;
+    }
+    n++;
+    s = t;
+  }
+  return n;
+}
+
+static long long count_tokens(const char* s, const char* end) {
+  long long n = 0;
+  bool in = false;
+  for (; s < end; s++) {
+    const bool w = is_ws(*s);
+    n += (!w && !in);
+    in = !w;
+  }
+  return n;
+}
+
+// src/io.cpp:132-161: the six header pairs, then ncols*nrows values, row 0 =
+// north.  The file is read in one piece and the values are converted in
+// parallel: the text is cut at whitespace into one chunk per thread, the
+// tokens of each chunk are counted, and each thread converts its chunk with
+// strtod (the correctly rounded conversion fscanf("%lf") performs) at its
+// offset, so the values are those of a sequential read.
 int read_dem(const char* path, int& ncols, int& nrows, double& xll, double& yll, double& cs,
              double& nodata, std::vector<double>& data) {
   FILE* fp = fopen(path, "rb");
   if (!fp) return AF_EIO;
   std::string buf;
-  {
-    char chunk[1 << 16];
-    size_t n;
-    while ((n = fread(chunk, 1, sizeof(chunk), fp)) > 0) buf.append(chunk, n);
-    fclose(fp);
+  if (fseek(fp, 0, SEEK_END) == 0) {
+    const long sz = ftell(fp);
+    if (sz > 0) {
+      buf.resize((size_t)sz);
+      rewind(fp);
+      if (fread(&buf[0], 1, (size_t)sz, fp) != (size_t)sz) {
+        fclose(fp);
+        return AF_EIO;
+      }
+    }
   }
+  fclose(fp);
   const char* s = buf.c_str();
   char* e = nullptr;
-  auto skip_ws = [&]() {
-    while (*s == ' ' || *s == '\t' || *s == '\n' || *s == '\r' || *s == '\v' || *s == '\f') s++;
-  };
   auto skip_word = [&]() {
-    skip_ws();
-    while (*s && !(*s == ' ' || *s == '\t' || *s == '\n' || *s == '\r' || *s == '\v' || *s == '\f'))
-      s++;
+    while (is_ws(*s)) s++;
+    while (*s && !is_ws(*s)) s++;
   };
   double hdr[6];
   for (int k = 0; k < 6; k++) {
@@ -154,14 +198,42 @@ int read_dem(const char* path, int& ncols, int& nrows, double& xll, double& yll,
   cs = hdr[4];
   nodata = hdr[5];
   if (ncols < 0 || nrows < 0) return AF_EIO;
-  const size_t n = (size_t)ncols * (size_t)nrows;
-  data.assign(n, 0.0);
-  for (size_t k = 0; k < n; k++) {
-    double v = strtod(s, &e);
-    if (e == s) return AF_EIO;
-    data[k] = v;
-    s = e;
+  const long long n = (long long)ncols * (long long)nrows;
+  data.assign((size_t)n, 0.0);
+  const char* end = buf.c_str() + buf.size();
+  int T = (int)std::min<unsigned>(32u, std::max(1u, std::thread::hardware_concurrency()));
+  if (end - s < (1 << 20)) T = 1;
+  // chunk boundaries at whitespace
+  std::vector<const char*> cut(T + 1, end);
+  cut[0] = s;
+  for (int t = 1; t < T; t++) {
+    const char* c = s + (end - s) * (long long)t / T;
+    while (c < end && !is_ws(*c)) c++;
+    cut[t] = std::max(c, cut[t - 1]);
   }
+  std::vector<long long> cnt(T, 0), off(T + 1, 0);
+  {
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; t++)
+      th.emplace_back([&, t] { cnt[t] = count_tokens(cut[t], cut[t + 1]); });
+    for (auto& x : th) x.join();
+  }
+  for (int t = 0; t < T; t++) off[t + 1] = off[t] + cnt[t];
+  if (off[T] < n) return AF_EIO;  // fewer values than the header announces
+  std::vector<int> bad(T, 0);
+  {
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; t++)
+      th.emplace_back([&, t] {
+        if (off[t] >= n) return;
+        const long long got =
+            parse_values(cut[t], cut[t + 1], data.data() + off[t], n - off[t]);
+        bad[t] = got < 0;
+      });
+    for (auto& x : th) x.join();
+  }
+  for (int t = 0; t < T; t++)
+    if (bad[t]) return AF_EIO;
   return AF_OK;
 }
 

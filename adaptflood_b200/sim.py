@@ -141,15 +141,17 @@ class Simulation:
             out["Vx"], out["Vy"] = self.velocity()
         return out
 
-    def depth(self) -> np.ndarray:
-        H = np.zeros(self.nx * self.ny)
+    def depth(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """H (FP64, reference layout); `out` may supply the array."""
+        H = np.zeros(self.nx * self.ny) if out is None else np.ascontiguousarray(out).reshape(-1)
+        assert H.size == self.nx * self.ny
         _lib.check(self.lib.af_sim_get_state(self.h, _p(H), None, None), "af_sim_get_state")
         return H.reshape(self.ny, self.nx)
 
     def set_state(self, H, Qx, Qy, t: float) -> None:
-        H = np.ascontiguousarray(H, dtype=np.float64)
-        Qx = np.ascontiguousarray(Qx, dtype=np.float64)
-        Qy = np.ascontiguousarray(Qy, dtype=np.float64)
+        """Sets the state and time; a field given as None keeps its current value."""
+        H, Qx, Qy = (None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                     for a in (H, Qx, Qy))
         _lib.check(self.lib.af_sim_set_state(self.h, _p(H), _p(Qx), _p(Qy), float(t)),
                    "af_sim_set_state")
 

@@ -145,3 +145,41 @@ def test_errors(tmp_path):
     with pytest.raises(_lib.AFError) as e:
         load_par(_minimal(tmp_path, "P 5 5 QVAR q\n", "t\nq\nx\n"))  # bad count line
     assert e.value.code == _lib.AF_EIO
+
+
+def test_large_dem_parsed_in_parallel_equals_sequential_values(tmp_path):
+    """Above 1 MB of text the DEM body is converted by several threads; the
+    values are the sequential reader's (round-trip text, formats of all kinds)."""
+    rng = np.random.default_rng(8)
+    ny, nx = 300, 410
+    dem = rng.normal(20.0, 5.0, size=(ny, nx))
+    dem[::7, ::5] = sc.NODATA
+    case = sc.Case(nx, ny, 2.0, dem, name="big")
+    par = case.write(str(tmp_path))
+    got, _ = load_par(par)
+    np.testing.assert_array_equal(got.dem, dem)
+    # hand-written text: mixed spacing, exponents, integers, line breaks anywhere
+    vals = rng.uniform(-50, 50, size=nx * ny)
+    toks = []
+    for k, v in enumerate(vals):
+        toks.append(("%.17g" if k % 3 else "%.6e") % v)
+    text = ("ncols %d\nnrows %d\nxllcorner 0\nyllcorner 0\ncellsize 1\nNODATA_value -9999\n"
+            % (nx, ny))
+    text += "".join(t + ("\n" if k % 97 == 0 else "  \t " if k % 5 == 0 else " ")
+                    for k, t in enumerate(toks))
+    path = tmp_path / "mixed.asc"
+    path.write_text(text)
+    want = np.array([float(t) for t in toks]).reshape(ny, nx)
+    case2 = sc.Case(nx, ny, 1.0, np.zeros((ny, nx)), name="mixed")
+    par2 = case2.write(str(tmp_path / "mixed_case"))
+    body = open(par2).read().replace(
+        "DEMfile " + str(tmp_path / "mixed_case" / "dem.asc"), "DEMfile " + str(path))
+    open(par2, "w").write(body)
+    got2, _ = load_par(par2)
+    np.testing.assert_array_equal(got2.dem, want)
+    # a malformed token deep in the body and a truncated body are errors
+    for bad in (text.replace(toks[nx * ny // 2], toks[nx * ny // 2] + "x", 1),
+                text[: len(text) * 3 // 4]):
+        path.write_text(bad)
+        with pytest.raises(_lib.AFError):
+            load_par(par2)
