@@ -1009,9 +1009,110 @@ static int run_output(Sim& s, double sim_time, const af_output_desc& o, int64_t*
   return writer.errors() ? AF_EIO : AF_OK;
 }
 
+// Checkpoint file: "AFCKPT01", int32 precision, nx, ny, mass count, the
+// control block (SimCtl, native layout), the mass series (3 doubles per
+// entry), then H (ny x nx), Qx (ny x (nx+1)) and Qy ((ny+1) x nx) in the state
+// precision, dense.  Native byte order: a checkpoint is read back on the same
+// kind of host it was written on.
+static const char kCkptMagic[8] = {'A', 'F', 'C', 'K', 'P', 'T', '0', '1'};
+
+static int field_io(Sim& s, DevBuf& b, std::vector<char>& host, int rows, int width, bool put) {
+  char* dev = static_cast<char*>(b.p) + (size_t)kGuard * s.esize;
+  const size_t w = (size_t)width * s.esize;
+  if (put)
+    AF_CUDA(cudaMemcpy2DAsync(dev, (size_t)s.P * s.esize, host.data(), w, w, rows,
+                              cudaMemcpyHostToDevice, s.st));
+  else
+    AF_CUDA(cudaMemcpy2DAsync(host.data(), w, dev, (size_t)s.P * s.esize, w, rows,
+                              cudaMemcpyDeviceToHost, s.st));
+  AF_CUDA(cudaStreamSynchronize(s.st));
+  return AF_OK;
+}
+
+static int checkpoint(Sim& s, const char* path) {
+  AF_CUDA(cudaSetDevice(s.device));
+  AF_TRY(read_ctl(s));
+  const SimCtl ctl = *s.pinned_ctl;
+  const int par = ctl.parity, nx = s.c.nx, ny = s.c.ny;
+  const int nm = std::min(ctl.mass_count, ctl.mass_cap);
+  std::vector<double> mass((size_t)nm * 3);
+  if (nm > 0) {
+    AF_CUDA(cudaMemcpyAsync(mass.data(), s.mass_series.p, mass.size() * 8, cudaMemcpyDeviceToHost,
+                            s.st));
+    AF_CUDA(cudaStreamSynchronize(s.st));
+  }
+  FILE* f = fopen(path, "wb");
+  if (!f) return AF_EIO;
+  std::unique_ptr<FILE, int (*)(FILE*)> guard(f, fclose);
+  const int32_t hdr[4] = {s.prec, nx, ny, nm};
+  bool ok = fwrite(kCkptMagic, 1, 8, f) == 8 && fwrite(hdr, sizeof hdr, 1, f) == 1 &&
+            fwrite(&ctl, sizeof ctl, 1, f) == 1 &&
+            (nm == 0 || fwrite(mass.data(), 8, mass.size(), f) == mass.size());
+  const int shape[3][2] = {{ny, nx}, {ny, nx + 1}, {ny + 1, nx}};
+  DevBuf* fields[3] = {&s.H[par], &s.Qx[par], &s.Qy[par]};
+  for (int k = 0; k < 3 && ok; k++) {
+    std::vector<char> host((size_t)shape[k][0] * shape[k][1] * s.esize);
+    AF_TRY(field_io(s, *fields[k], host, shape[k][0], shape[k][1], false));
+    ok = fwrite(host.data(), 1, host.size(), f) == host.size();
+  }
+  guard.reset();
+  return ok ? AF_OK : AF_EIO;
+}
+
+static int restore(Sim& s, const char* path) {
+  AF_CUDA(cudaSetDevice(s.device));
+  FILE* f = fopen(path, "rb");
+  if (!f) return AF_EIO;
+  std::unique_ptr<FILE, int (*)(FILE*)> guard(f, fclose);
+  char magic[8];
+  int32_t hdr[4];
+  SimCtl ctl;
+  if (fread(magic, 1, 8, f) != 8 || memcmp(magic, kCkptMagic, 8) != 0 ||
+      fread(hdr, sizeof hdr, 1, f) != 1 || fread(&ctl, sizeof ctl, 1, f) != 1)
+    return AF_EIO;
+  const int nx = s.c.nx, ny = s.c.ny;
+  if (hdr[0] != s.prec || hdr[1] != nx || hdr[2] != ny || hdr[3] < 0 || hdr[3] > kMassCap ||
+      ctl.parity < 0 || ctl.parity > 1)
+    return AF_EINVAL;  // another case or precision
+  std::vector<double> mass((size_t)hdr[3] * 3);
+  if (!mass.empty() && fread(mass.data(), 8, mass.size(), f) != mass.size()) return AF_EIO;
+  const int par = ctl.parity;
+  const int shape[3][2] = {{ny, nx}, {ny, nx + 1}, {ny + 1, nx}};
+  DevBuf* fields[3] = {&s.H[par], &s.Qx[par], &s.Qy[par]};
+  std::vector<std::vector<char>> host(3);
+  for (int k = 0; k < 3; k++) {
+    host[k].resize((size_t)shape[k][0] * shape[k][1] * s.esize);
+    if (fread(host[k].data(), 1, host[k].size(), f) != host[k].size()) return AF_EIO;
+  }
+  for (int k = 0; k < 3; k++) AF_TRY(field_io(s, *fields[k], host[k], shape[k][0], shape[k][1], true));
+  if (!mass.empty()) {
+    AF_CUDA(cudaMemcpyAsync(s.mass_series.p, mass.data(), mass.size() * 8, cudaMemcpyHostToDevice,
+                            s.st));
+    AF_CUDA(cudaStreamSynchronize(s.st));
+  }
+  ctl.mass_count = hdr[3];
+  ctl.mass_cap = kMassCap;
+  ctl.hmax_acc = ord_encode(-DBL_MAX);
+  ctl.arrive = 0;
+  ctl.done = 1;
+  ctl.status = 0;
+  *s.pinned_ctl = ctl;
+  return write_ctl(s);
+}
+
 }  // namespace af
 
 extern "C" {
+
+int af_sim_checkpoint(af_sim* h, const char* path) {
+  if (!h || !path) return AF_EINVAL;
+  return af::checkpoint(*h->s, path);
+}
+
+int af_sim_restore(af_sim* h, const char* path) {
+  if (!h || !path) return AF_EINVAL;
+  return af::restore(*h->s, path);
+}
 
 int af_sim_run_output(af_sim* h, double sim_time, const af_output_desc* o, int64_t* steps) {
   if (!h || !o) return AF_EINVAL;

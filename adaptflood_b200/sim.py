@@ -194,6 +194,14 @@ class Simulation:
         del keep
         return n.value
 
+    def checkpoint(self, path: str) -> None:
+        """Writes the whole state to a binary checkpoint (af_sim_checkpoint)."""
+        _lib.check(self.lib.af_sim_checkpoint(self.h, os.fsencode(path)), "af_sim_checkpoint")
+
+    def restore(self, path: str) -> None:
+        """Loads a checkpoint of the same case and precision (af_sim_restore)."""
+        _lib.check(self.lib.af_sim_restore(self.h, os.fsencode(path)), "af_sim_restore")
+
     def mass_series(self):
         n = C.c_int()
         _lib.check(self.lib.af_sim_mass_series(self.h, None, None, None, 0, C.byref(n)),

@@ -223,6 +223,15 @@ int af_sim_volume(af_sim* s, double* vol, double* area);
  * (src/main.cpp:291-304): up to cap entries of (t, vol, area). */
 int af_sim_mass_series(af_sim* s, double* t, double* vol, double* area, int cap, int* n);
 
+/* Checkpoint and restart (no counterpart in the reference, which always starts
+ * at t = 0): af_sim_checkpoint writes the whole simulation state (fields in the
+ * state precision, time, step count, dt inputs, rain rate, mass-report series)
+ * to a binary file; af_sim_restore loads it into a simulation created from the
+ * same case and precision (AF_EINVAL otherwise), after which the run continues
+ * bit for bit as if it had never stopped.  Files use the host's byte order. */
+int af_sim_checkpoint(af_sim* s, const char* path);
+int af_sim_restore(af_sim* s, const char* path);
+
 /* Output of a run as the reference's main loop writes it (src/main.cpp:196-388,
  * src/io.cpp:314-334, src/async_output.cpp:84-176): ESRI ASCII grids with
  * "%.4f " values in out_dir (created if missing): H_0000.asc for the state at

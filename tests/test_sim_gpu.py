@@ -12,6 +12,7 @@ import pytest
 from _util import golden_names, load_golden
 from adaptflood_b200 import forcing as fc
 from adaptflood_b200 import scenarios as sc
+from adaptflood_b200._lib import AFError
 from adaptflood_b200.sim import Simulation
 from oracle import oracle as orc
 
@@ -273,3 +274,34 @@ def test_fp32_rain_on_deep_water_conserves_mass(cuda):
     added = 0.5e-3 / 3600.0 * t * case.cells * case.dx ** 2
     assert abs(vols["f64"] - (v0 + added)) <= 1e-9 * v0
     assert abs(vols["f32"] - vols["f64"]) <= FP32_MASS_TOL * vols["f64"]
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_checkpoint_restart_is_bit_identical(cuda, tmp_path, prec):
+    case = sc.small_case(131, 77, seed=61, rain=True, n_hvar=1, n_qvar=2, sim_time=400.0)
+    f = fc.pack(case)
+    ck = str(tmp_path / "run.ckpt")
+    with Simulation(case, prec, forcing=f) as a:
+        a.run(150.0)
+        a.checkpoint(ck)
+        a.run(case.sim_time)
+        ref, ref_mass, ref_status = a.state(), a.mass_series(), a.status()
+    with Simulation(case, prec, forcing=f) as b:
+        b.restore(ck)
+        b.run(case.sim_time)
+        st, mass, status = b.state(), b.mass_series(), b.status()
+    assert status == ref_status
+    for k in ("H", "Qx", "Qy"):
+        np.testing.assert_array_equal(st[k], ref[k])
+    for x, y in zip(mass, ref_mass):
+        np.testing.assert_array_equal(x, y)
+    other = "f32" if prec == "f64" else "f64"
+    with Simulation(case, other, forcing=f) as c:
+        with pytest.raises(AFError):
+            c.restore(ck)
+    small = sc.small_case(40, 30, seed=62, sim_time=100.0)
+    with Simulation(small, prec) as d:
+        with pytest.raises(AFError):
+            d.restore(ck)
+        with pytest.raises(AFError):
+            d.restore(str(tmp_path / "missing.ckpt"))
