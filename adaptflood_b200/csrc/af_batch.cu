@@ -146,6 +146,7 @@ struct Batch {
   cudaStream_t st = nullptr, cst = nullptr;
   char* arena = nullptr;
   Arena plan;
+  double* stage = nullptr;  // kStageBytes of FP64 staging for FP32 field transfers
   BatchScen* d_scen = nullptr;
   SimCtl* d_ctl = nullptr;
   BatchTab* d_tab = nullptr;
@@ -176,6 +177,7 @@ struct Batch {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (arena) cudaFree(arena);
+    if (stage) cudaFree(stage);
     if (d_scen) cudaFree(d_scen);
     if (d_ctl) cudaFree(d_ctl);
     if (d_tab) cudaFree(d_tab);
@@ -286,6 +288,7 @@ static int create(int precision, int device, uint64_t arena_bytes, int variant, 
   AF_CUDA(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
   AF_CUDA(cudaStreamCreateWithFlags(&b->cst, cudaStreamNonBlocking));
   AF_TRY(alloc_dev((void**)&b->arena, arena_bytes));
+  AF_TRY(alloc_dev((void**)&b->stage, kStageBytes));
   b->plan.reset(arena_bytes);
   AF_TRY(alloc_dev((void**)&b->d_scen, sizeof(BatchScen) * kMaxSlots));
   AF_TRY(alloc_dev((void**)&b->d_ctl, sizeof(SimCtl) * kMaxSlots));
@@ -328,13 +331,28 @@ static int put_vec(Batch& b, char* base, size_t off, const std::vector<V>& v) {
   return AF_OK;
 }
 
+// Caller FP64 rows -> a padded field in the arena (`dst` = the field's
+// allocation, front guard included), on the copy stream: FP64 in one 2-D copy,
+// FP32 through the staging buffer and a conversion kernel.
 template <typename T>
-static int put_padded(Batch& b, char* dst, const double* src, int rows, int width, int P,
-                      size_t elems) {
-  std::vector<T> img(elems, T(0));
-  pad_field<T>(src, rows, width, (size_t)width, P, img.data());
-  AF_CUDA(cudaMemcpyAsync(dst, img.data(), elems * sizeof(T), cudaMemcpyHostToDevice, b.cst));
-  AF_CUDA(cudaStreamSynchronize(b.cst));  // the image is a temporary
+static int put_padded(Batch& b, char* dst, const double* src, int rows, int width, int P) {
+  T* d = reinterpret_cast<T*>(dst) + kGuard;
+  if (sizeof(T) == 8) {
+    AF_CUDA(cudaMemcpy2DAsync(d, (size_t)P * 8, src, (size_t)width * 8, (size_t)width * 8, rows,
+                              cudaMemcpyHostToDevice, b.cst));
+  } else {
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(rows, kStageBytes / (8 * (size_t)width)));
+    for (int j = 0; j < rows; j += chunk) {
+      const int n = std::min(chunk, rows - j);
+      AF_CUDA(cudaMemcpy2DAsync(b.stage, (size_t)width * 8, src + (size_t)j * width,
+                                (size_t)width * 8, (size_t)width * 8, n, cudaMemcpyHostToDevice,
+                                b.cst));
+      k_pad_from_f64<<<grid_for((long long)n * width, 256, 8), 256, 0, b.cst>>>(
+          b.stage, n, width, reinterpret_cast<float*>(d) + (size_t)j * P, P);
+      AF_CUDA(cudaGetLastError());
+    }
+  }
+  AF_CUDA(cudaStreamSynchronize(b.cst));
   return AF_OK;
 }
 
@@ -362,16 +380,15 @@ static int add(Batch& b, const af_case_desc* c, const af_forcing_desc* f, const 
   HostTables tb;
   build_tables(c, f, 30 * b.N, R, L.nsx, L.nsy, tb);
   char* base = b.arena + off;
-  const size_t ce = cell_elems(L.ny, L.P);
   int rc = AF_OK;
   if (cudaMemsetAsync(base, 0, L.total, b.cst) != cudaSuccess)
     return fail(cuda_fail(cudaGetLastError()));
   if (b.prec == AF_PREC_F64) {
-    rc = put_padded<double>(b, base + L.DEM, dem, L.ny, L.nx, L.P, ce);
-    if (rc == AF_OK && h0) rc = put_padded<double>(b, base + L.H[0], h0, L.ny, L.nx, L.P, ce);
+    rc = put_padded<double>(b, base + L.DEM, dem, L.ny, L.nx, L.P);
+    if (rc == AF_OK && h0) rc = put_padded<double>(b, base + L.H[0], h0, L.ny, L.nx, L.P);
   } else {
-    rc = put_padded<float>(b, base + L.DEM, dem, L.ny, L.nx, L.P, ce);
-    if (rc == AF_OK && h0) rc = put_padded<float>(b, base + L.H[0], h0, L.ny, L.nx, L.P, ce);
+    rc = put_padded<float>(b, base + L.DEM, dem, L.ny, L.nx, L.P);
+    if (rc == AF_OK && h0) rc = put_padded<float>(b, base + L.H[0], h0, L.ny, L.nx, L.P);
   }
   if (rc != AF_OK) return fail(rc);
   const int puts[] = {
@@ -613,15 +630,26 @@ static bool finished(const Batch& b, int slot) {
   return c.status != 0 || !(c.t < c.t_stop) || c.step >= c.step_stop;
 }
 
+// A padded field (first element at src) -> caller FP64 rows at host pitch
+// hpitch, on the copy stream; FP32 is converted on the device first.
 template <typename T>
 static int get_field(Batch& b, const char* src, int rows, int width, int P, double* dst,
                      size_t hpitch) {
-  std::vector<T> tmp((size_t)rows * width);
-  AF_CUDA(cudaMemcpy2DAsync(tmp.data(), (size_t)width * sizeof(T), src, (size_t)P * sizeof(T),
-                            (size_t)width * sizeof(T), rows, cudaMemcpyDeviceToHost, b.cst));
+  if (sizeof(T) == 8) {
+    AF_CUDA(cudaMemcpy2DAsync(dst, hpitch * 8, src, (size_t)P * 8, (size_t)width * 8, rows,
+                              cudaMemcpyDeviceToHost, b.cst));
+  } else {
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(rows, kStageBytes / (8 * (size_t)width)));
+    for (int j = 0; j < rows; j += chunk) {
+      const int n = std::min(chunk, rows - j);
+      k_dense_to_f64<<<grid_for((long long)n * width, 256, 8), 256, 0, b.cst>>>(
+          reinterpret_cast<const float*>(src) + (size_t)j * P, P, n, width, b.stage);
+      AF_CUDA(cudaGetLastError());
+      AF_CUDA(cudaMemcpy2DAsync(dst + (size_t)j * hpitch, hpitch * 8, b.stage, (size_t)width * 8,
+                                (size_t)width * 8, n, cudaMemcpyDeviceToHost, b.cst));
+    }
+  }
   AF_CUDA(cudaStreamSynchronize(b.cst));
-  for (int j = 0; j < rows; j++)
-    for (int i = 0; i < width; i++) dst[(size_t)j * hpitch + i] = (double)tmp[(size_t)j * width + i];
   return AF_OK;
 }
 

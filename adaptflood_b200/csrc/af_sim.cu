@@ -314,27 +314,6 @@ static int alloc_field(DevBuf& b, size_t elems, int esize) {
 // one 2-D copy.  FP32 fields go through a dense FP64 device staging buffer in
 // chunks of rows, converted by a kernel on the device, so the host does no
 // per-element work (and pinned host arrays move at full link bandwidth).
-__global__ void k_pad_from_f64(const double* __restrict__ src, int rows, int width,
-                               float* __restrict__ dst, int P) {
-  const long long n = (long long)rows * width;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-       k += (long long)gridDim.x * blockDim.x) {
-    const long long j = k / width, i = k - j * width;
-    dst[j * P + i] = (float)src[k];
-  }
-}
-__global__ void k_dense_to_f64(const float* __restrict__ src, int P, int rows, int width,
-                               double* __restrict__ dst) {
-  const long long n = (long long)rows * width;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-       k += (long long)gridDim.x * blockDim.x) {
-    const long long j = k / width, i = k - j * width;
-    dst[k] = (double)src[j * P + i];
-  }
-}
-
-constexpr size_t kStageBytes = 64u << 20;
-
 static int put_field(Sim& s, DevBuf& b, const double* src, int rows, int width, size_t hpitch) {
   char* dst = static_cast<char*>(b.p) + (size_t)kGuard * s.esize;
   if (s.prec == AF_PREC_F64) {

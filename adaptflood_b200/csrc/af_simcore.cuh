@@ -70,17 +70,6 @@ int check_case(const af_case_desc* c, const af_forcing_desc* f);
 void build_tables(const af_case_desc* c, const af_forcing_desc* f, int own, int R, int nsx,
                   int nsy, HostTables& t);
 
-// Copies `rows` x `width` FP64 values (host pitch hpitch) into a padded host
-// image of a field in precision T (rows of pitch P, front guard kGuard).
-template <typename T>
-void pad_field(const double* src, int rows, int width, size_t hpitch, int P, T* dst) {
-  for (int j = 0; j < rows; j++) {
-    T* d = dst + kGuard + (size_t)j * P;
-    const double* s = src + (size_t)j * hpitch;
-    for (int i = 0; i < width; i++) d[i] = (T)s[i];
-  }
-}
-
 // ------------------------------------------------------------- kernels
 template <typename T>
 __global__ void k_hmax_int(const T* __restrict__ H, const T* __restrict__ Z, int nx, int ny,
@@ -163,6 +152,30 @@ __global__ void k_volume_int(const T* __restrict__ H, int nx, int ny, int P, dou
     part[3 * blockIdx.x] = S;
     part[3 * blockIdx.x + 1] = C;
     part[3 * blockIdx.x + 2] = A;
+  }
+}
+
+// Dense FP64 rows <-> a padded FP32 field (pitch P), converted on the device:
+// transfers of FP32 state move the caller's FP64 values through a device
+// staging buffer in chunks, with no per-element host work.
+constexpr size_t kStageBytes = 64u << 20;
+
+static __global__ void k_pad_from_f64(const double* __restrict__ src, int rows, int width,
+                               float* __restrict__ dst, int P) {
+  const long long n = (long long)rows * width;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const long long j = k / width, i = k - j * width;
+    dst[j * P + i] = (float)src[k];
+  }
+}
+static __global__ void k_dense_to_f64(const float* __restrict__ src, int P, int rows, int width,
+                               double* __restrict__ dst) {
+  const long long n = (long long)rows * width;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const long long j = k / width, i = k - j * width;
+    dst[k] = (double)src[j * P + i];
   }
 }
 

@@ -276,6 +276,117 @@ def time_e2e(case, forcing, precision, steps, device):
     return case.cells * steps / el, h2d // steps, H.nbytes // steps
 
 
+def _event_timer(stream_ptr, device):
+    import torch
+    stream = torch.cuda.ExternalStream(stream_ptr, device=device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    return stream, e0, e1
+
+
+def run_ensemble(args, device, peak):
+    """C4: the ensemble in one batch (FP32 state, FP64 time/mass), every
+    scenario from t = 0 to its sim_time, one timed launch of the batch loop;
+    beside it a sample of the same scenarios on the plain FP64 single-grid
+    path, one at a time."""
+    import torch
+    from adaptflood_b200.batch import Batch, size_class
+    from adaptflood_b200.sim import Simulation
+    from adaptflood_b200.tune import tune_rows
+    cases = sc.config4(count=args.ensemble)
+    forcings = [fc.pack(c) for c in cases]
+    classes = sorted({size_class(c.nx, c.ny) for c in cases})
+    t0 = time.perf_counter()
+    rows = tune_rows(classes, "f32", device=device)
+    tune_s = time.perf_counter() - t0
+    with Batch("f32", device=device, rows=rows) as b:
+        need = sum(b.footprint(c, f) for c, f in zip(cases, forcings))
+        slots = [b.add(c, f) for c, f in zip(cases, forcings)]
+        stream, e0, e1 = _event_timer(b.stream, device)
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        b.launch()
+        e1.record(stream)
+        b.sync()
+        ms = e0.elapsed_time(e1)
+        steps = [b.status(s)[3] for s in slots]
+        batch_steps = b.info()["batch_steps"]
+    cu = sum(c.cells * n for c, n in zip(cases, steps))
+    value = cu / (ms / 1e3)
+    ach = BYTES_PER_CELL["f32"] * value / 1e9
+    # plain FP64 path on a sample spread over the size range
+    order = sorted(range(len(cases)), key=lambda k: cases[k].cells)
+    pick = [order[int(round(q * (len(order) - 1) / max(1, args.fp64_sample - 1)))]
+            for q in range(min(args.fp64_sample, len(order)))]
+    cu64 = 0
+    ms64 = 0.0
+    for k in pick:
+        with Simulation(cases[k], "f64", device=device, forcing=forcings[k]) as s:
+            st, a0, a1 = _event_timer(s.stream, device)
+            torch.cuda.synchronize(device)
+            a0.record(st)
+            s.launch(cases[k].sim_time)
+            a1.record(st)
+            s.sync()
+            ms64 += a0.elapsed_time(a1)
+            cu64 += cases[k].cells * s.steps
+    v64 = cu64 / (ms64 / 1e3)
+    return {
+        "workload": f"C4 ensemble: {len(cases)} scenarios, grids log-uniform 256^2..2048^2 "
+                    f"(aspect 1:1..1:4, dx 2/5/10 m), n U(0.02,0.08), 1-64 QFIX/QVAR, all "
+                    f"edges FREE, each from t=0 to sim_time 1800 s in one batch",
+        "cells": sum(c.cells for c in cases), "cell_updates": cu, "batch_steps": batch_steps,
+        "scenario_steps": [min(steps), int(np.median(steps)), max(steps)],
+        "seconds": ms / 1e3, "value": value, "unit": "cell-updates/s",
+        "scenarios_per_s": len(cases) / (ms / 1e3), "dtype": "f32",
+        "arena_bytes_used": need,
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                     "frac": ach / peak, "algorithmic_bytes_per_cell": BYTES_PER_CELL["f32"],
+                     "note": "whole batch loop (graph launch incl. begin kernel and the tail "
+                             "where few scenarios remain) / wall time on the device"},
+        "tuned_rows": {str(k): v for k, v in rows.items()}, "tune_seconds": tune_s,
+        "plain_fp64": {"value": v64, "unit": "cell-updates/s", "scenarios": len(pick),
+                       "path": "Simulation f64, one scenario at a time, CUDA events around "
+                               "each run"},
+        "batched_fp32_over_plain_fp64": value / v64,
+    }
+
+
+def run_serving(args, device):
+    """C5: Poisson request streams served by continuous batching (FP32, FP64
+    accumulators), latency from arrival to the depth field on the host;
+    beside it the plain FP64 path serving the same stream one at a time."""
+    from adaptflood_b200.batch import size_class
+    from adaptflood_b200.serve import Request, Server, poisson_arrivals, serve_one_at_a_time
+    from adaptflood_b200.serve import summary
+    from adaptflood_b200.tune import tune_rows
+    cases = sc.config5(count=args.serve_requests)
+    forcings = [fc.pack(c) for c in cases]
+    rows = tune_rows(sorted({size_class(c.nx, c.ny) for c in cases}), "f32", device=device)
+    rates = [float(x) for x in args.serve_rates.split(",") if x]
+    out = {"workload": f"C5 served loop: {len(cases)} requests per rate, grids log-uniform "
+                       f"128^2..4096^2, sim_time U(600,3600) s, Poisson arrivals",
+           "rates": {}}
+    for rate in rates:
+        rng = np.random.default_rng(int(rate * 1000) + 7)
+        arr = poisson_arrivals(rate, len(cases), rng)
+        reqs = [Request(k, float(arr[k]), cases[k], forcings[k]) for k in range(len(cases))]
+        with Server("f32", device=device, rows=rows, keep_results=False) as srv:
+            srv.run(reqs)
+            launches = srv.launches
+        sm = summary(reqs)
+        sm["launches"] = launches
+        out["rates"][str(rate)] = sm
+    # the plain FP64 path, one request at a time, at the middle rate
+    rate = rates[len(rates) // 2]
+    rng = np.random.default_rng(int(rate * 1000) + 7)
+    arr = poisson_arrivals(rate, len(cases), rng)
+    reqs = [Request(k, float(arr[k]), cases[k], forcings[k]) for k in range(len(cases))]
+    serve_one_at_a_time(reqs, "f64", device=device, keep_results=False)
+    out["plain_fp64_one_at_a_time"] = dict(summary(reqs), rate=rate)
+    return out
+
+
 def traffic_per_cell(kernel_key: str):
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
