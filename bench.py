@@ -267,13 +267,19 @@ def time_e2e(case, forcing, precision, steps, device):
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
     s = Simulation(c, precision, device=device, forcing=forcing)
+    t1 = time.perf_counter()
     s.set_state(None, None, None, T_START)
+    t2 = time.perf_counter()
     s.run(1e30, max_steps=steps)
+    t3 = time.perf_counter()
     H = s.depth(out=out)
-    el = time.perf_counter() - t0
+    t4 = time.perf_counter()
+    el = t4 - t0
     s.close()
     h2d = c.dem.nbytes + c.h0.nbytes + sum(a.nbytes for a in forcing.__dict__.values())
-    return case.cells * steps / el, h2d // steps, H.nbytes // steps
+    phases = {"create_s": t1 - t0, "set_time_s": t2 - t1, "steps_s": t3 - t2,
+              "readback_s": t4 - t3}
+    return case.cells * steps / el, h2d // steps, H.nbytes // steps, phases
 
 
 def _event_timer(stream_ptr, device):
@@ -439,8 +445,8 @@ def run_ours(args, rank: int, world: int):
     ach64 = BYTES_PER_CELL["f64"] * cells / (step_ms64 / 1e3) / 1e9
     tr32 = traffic_per_cell("k_step_f32")
     tr64 = traffic_per_cell("k_step_f64")
-    e2e_v, h2d, d2h = (0.0, 0, 0) if args.no_e2e else time_e2e(case, forcing, "f32", args.steps,
-                                                                 local)
+    e2e_v, h2d, d2h, phases = ((0.0, 0, 0, {}) if args.no_e2e else
+                               time_e2e(case, forcing, "f32", args.steps, local))
     if dist is not None:
         t = torch.tensor([e2e_v], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MIN)
@@ -473,7 +479,8 @@ def run_ours(args, rank: int, world: int):
             "e2e": {"value": e2e_v, "unit": "cell-updates/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h),
                     "path": "af_sim_create (DEM, start depth, forcing) from pinned host arrays, "
-                            "K steps, af_sim_get_state of the depth field into pinned host memory"},
+                            "K steps, af_sim_get_state of the depth field into pinned host memory",
+                    "phases": phases},
             "gpu_launches": args.steps + 1,
             "clocks": clk.summary(),
             "state_after": {"f32": info32, "f64": info64},
