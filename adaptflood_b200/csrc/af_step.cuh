@@ -1002,22 +1002,31 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
 //     time read adjacent 512-byte segments of the same rows.  A unit ends
 //     with a fire-and-forget atomicMax of its Hmax and, at mass-report steps,
 //     a store of its volume partials; nothing waits.
+//     A warp fetches the record of its next unit's scenario (one bulk copy
+//     into the second of its two record buffers) while it runs the current
+//     unit, so switching scenarios between units costs no wait.
 //   k_batch_fold (one block): folds every active scenario's step (a thread
 //     per scenario; a warp per volume sum at mass-report steps), writes the
-//     scenario's next dt, time and parity beside its parameters, rebuilds the
-//     active list when a scenario has finished, and sets the loop condition.
+//     scenario's next dt, time, parity and step constants beside its
+//     parameters, rebuilds the active list when a scenario has finished, and
+//     sets the loop condition.
 // A scenario's results do not depend on which other scenarios share the
 // batch: every face and cell is computed by the same code, Hmax is an exact
 // max, and its volume partials are summed per strip in strip order.
 constexpr int kMaxSlots = 1024;
 constexpr int kFoldThreads = 1024;  // one block of the fold and begin kernels
 
-// Per slot: the scenario's parameters and its coming step.
-struct BatchScen {
+// Per slot: the scenario's parameters and its coming step.  Copied whole
+// into shared memory by one bulk copy (16-byte size and alignment).
+struct __align__(16) BatchScen {
   StepParams p;
   double t, dt, rate, next_mass;  // written by the begin and fold kernels
   int parity, pad;
+  // The coming step's StepScal<T> (T: the batch's precision), written with t.
+  __align__(16) unsigned char scal[sizeof(StepScal<double>)];
 };
+static_assert(sizeof(BatchScen) % 16 == 0, "bulk-copied record");
+static_assert(sizeof(StepScal<float>) <= sizeof(StepScal<double>), "scalar storage");
 
 struct BatchTab {
   int nmember;                // slots in the batch (written by the host)
@@ -1086,7 +1095,8 @@ __device__ inline void batch_compact(const BatchParams& bp) {
   }
 }
 
-// The coming step of one scenario, from its control block.
+// The coming step of one scenario, from its control block, and its constants.
+template <typename T>
 __device__ inline void batch_next(BatchScen* s) {
   const SimCtl* c = s->p.ctl;
   s->t = c->t;
@@ -1094,6 +1104,8 @@ __device__ inline void batch_next(BatchScen* s) {
   s->rate = c->rain_rate;
   s->next_mass = c->next_mass;
   s->parity = c->parity;
+  fill_scalars(s->p, s->t, s->dt, s->rate, s->next_mass, s->parity,
+               *reinterpret_cast<StepScal<T>*>(s->scal));
 }
 
 // Sets up one launch of the batch loop: the step limit, the active list,
@@ -1107,7 +1119,7 @@ __global__ void __launch_bounds__(kFoldThreads) k_batch_begin(const BatchParams 
   if (threadIdx.x < 32) batch_compact(bp);
   __syncthreads();
   const int nact = tab->nact;
-  for (int a = threadIdx.x; a < nact; a += blockDim.x) batch_next(&bp.scen[tab->act[a]]);
+  for (int a = threadIdx.x; a < nact; a += blockDim.x) batch_next<T>(&bp.scen[tab->act[a]]);
   if (threadIdx.x == 0) {
     const long long s = b->step;
     b->step_stop = (max_steps > (long long)0x3FFFFFFFFFFFFFFFLL - s) ? 0x3FFFFFFFFFFFFFFFLL
@@ -1169,7 +1181,7 @@ __global__ void __launch_bounds__(kFoldThreads) k_batch_fold(const BatchParams b
                   mass ? s_area[a] : 0.0))
       done++;
     else
-      batch_next(s);
+      batch_next<T>(s);
   }
   const int ndone = __syncthreads_count(done);
   if (ndone > 0) {  // the active list changes only when a scenario finishes
@@ -1194,52 +1206,71 @@ __global__ void __launch_bounds__(kFoldThreads) k_batch_fold(const BatchParams b
 template <typename T, int WY, int MINB>
 __global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams bp) {
   __shared__ __align__(128) unsigned char s_ring[WY][kStages][4][kRowBytes];
-  __shared__ __align__(8) uint64_t s_bar[WY][kStages];
-  __shared__ __align__(16) BatchScen s_scen[WY];
-  __shared__ __align__(16) StepScal<T> s_sc[WY];
+  __shared__ __align__(8) uint64_t s_bar[WY][kStages + 1];  // the ring's, then the records'
+  __shared__ BatchScen s_rec[WY][2];
   if (*(volatile int*)&bp.bctl->done) return;
   const BatchTab* tab = bp.tab;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   uint64_t* bar = s_bar[warp];
+  uint64_t* rbar = &s_bar[warp][kStages];
   if (lane == 0) {
-    for (int s = 0; s < kStages; s++) mbar_init(&bar[s], 1);
+    for (int s = 0; s <= kStages; s++) mbar_init(&bar[s], 1);
     fence_mbar_init();
   }
   __syncwarp();
   int kglob = 0;
+  uint32_t rphase = 0;  // completed record fetches, mod 2
   const int units = tab->units;
   const int nact = tab->nact;
   const int W = gridDim.x * WY;
-  int a = 0;     // active-scenario index of the current unit (only grows)
-  int cur = -1;  // slot whose record is in s_scen[warp] and s_sc[warp]
-  const StepParams& p = s_scen[warp].p;
-  StepScal<T>& sc = s_sc[warp];
-  for (int u = blockIdx.x * WY + warp; u < units; u += W) {
-    for (;;) {  // u0 is increasing: count the entries past `a` that are <= u
+  // Active-scenario index of unit u, from the index `a` of an earlier unit
+  // (u0 is increasing: count the entries past `a` that are <= u).
+  auto scen_of = [&](int a, int u) {
+    for (;;) {
       const int idx = a + 1 + lane;
       const bool le = idx < nact && tab->u0[idx] <= u;
       const unsigned m = __ballot_sync(0xffffffffu, le);
       a += __popc(m);
-      if (m != 0xffffffffu) break;
+      if (m != 0xffffffffu) return a;
     }
-    const int slot = tab->act[a];
-    if (slot != cur) {  // one parallel load of the scenario's record
-      __syncwarp();
-      const int* src = reinterpret_cast<const int*>(&bp.scen[slot]);
-      int* dst = reinterpret_cast<int*>(&s_scen[warp]);
-      for (int i = lane; i < (int)(sizeof(BatchScen) / 4); i += 32) dst[i] = src[i];
-      __syncwarp();
-      cur = slot;
-      if (lane == 0) {
-        const BatchScen& r = s_scen[warp];
-        fill_scalars(p, r.t, r.dt, r.rate, r.next_mass, r.parity, sc);
-      }
-      __syncwarp();
+  };
+  // One bulk copy of a slot's record into buffer `b` (the warp has finished
+  // reading that buffer: every lane has passed a __syncwarp since).
+  auto fetch = [&](int slot, int b) {
+    if (lane == 0) {
+      mbar_expect_tx(rbar, (uint32_t)sizeof(BatchScen));
+      fence_proxy_async();
+      bulk_g2s(&s_rec[warp][b], &bp.scen[slot], (uint32_t)sizeof(BatchScen), rbar);
     }
+  };
+  auto fetched = [&]() {
+    const bool ok = mbar_wait_warp(rbar, rphase);
+    rphase ^= 1u;
+    return ok;
+  };
+  int u = blockIdx.x * WY + warp;
+  if (u >= units) return;
+  int a = scen_of(0, u);
+  int slot = tab->act[a];
+  int buf = 0;
+  fetch(slot, buf);
+  bool ok = fetched();
+  if (!ok) mbar_wait_warp(rbar, rphase ^ 1u);  // drain the copy before leaving
+  while (ok) {
+    // The next unit's scenario; its record is fetched while this unit runs.
+    const int un = u + W;
+    const int an = un < units ? scen_of(a, un) : a;
+    const int slot_n = un < units ? tab->act[an] : -1;
+    const bool refetch = slot_n >= 0 && slot_n != slot;
+    __syncwarp();
+    if (refetch) fetch(slot_n, buf ^ 1);
+    const BatchScen& rec = s_rec[warp][buf];
+    const StepParams& p = rec.p;
+    const StepScal<T>& sc = *reinterpret_cast<const StepScal<T>*>(rec.scal);
     const int k = u - tab->u0[a];
     LaneAcc<T> acc{T(-FLT_MAX), 0.0, 0.0};
-    const bool ok = run_strip<T>(p, sc, k % p.nsx, k / p.nsx, s_ring[warp], bar, kglob, acc);
+    ok = run_strip<T>(p, sc, k % p.nsx, k / p.nsx, s_ring[warp], bar, kglob, acc);
     double m = acc.any_cell() ? (double)acc.m_cell : -DBL_MAX;
     m = warp_maxd(m);
     double v = 0.0, ar = 0.0;
@@ -1255,12 +1286,21 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams 
         p.partials[3 * k + 2] = ar;
       }
     }
-    if (!ok) {
-      // A wait timed out: this step's state is incomplete, so stop the batch.
-      if (lane == 0) atomicExch(&bp.bctl->status, 1);
-      break;
+    if (refetch) {
+      // Waited for even after a failure: no copy may be in flight at exit.
+      if (!fetched()) {
+        mbar_wait_warp(rbar, rphase ^ 1u);
+        ok = false;
+      }
+      buf ^= 1;
     }
+    if (slot_n < 0) break;
+    u = un;
+    a = an;
+    slot = slot_n;
   }
+  // A wait timed out: this step's state is incomplete, so stop the batch.
+  if (!ok && lane == 0) atomicExch(&bp.bctl->status, 1);
 }
 
 // Kernel entry points of the two precisions (defined in af_step_f64.cu and
