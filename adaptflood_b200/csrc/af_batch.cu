@@ -274,9 +274,10 @@ static int create(int precision, int device, uint64_t arena_bytes, int variant, 
   b->esize = precision == AF_PREC_F64 ? 8 : 4;
   b->N = 16 / b->esize;
   if (variant < 0) {
-    // Default: 1 warp per block, 12 resident blocks per SM (168 registers, no
-    // spills; the 16-block shape spills scenario parameters held in registers).
-    variant = 1;
+    // Default: 1 warp per block with 16 resident blocks per SM in FP32 (128
+    // registers, no spills: the fastest shape on every measured mix), 12 in
+    // FP64 (whose 16-block shape spills).
+    variant = precision == AF_PREC_F32 ? 0 : 1;
     if (const char* v = getenv("AF_BATCH_VARIANT")) variant = atoi(v);
   }
   if (variant < 0 || variant >= kStepVariants) return AF_EINVAL;

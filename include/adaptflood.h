@@ -294,7 +294,7 @@ typedef struct af_batch af_batch;
 
 /* precision: AF_PREC_F32 or AF_PREC_F64.  variant: launch shape of the batch
  * step kernel (0..4: warps per block x resident blocks per SM = 1x16, 1x12,
- * 1x20, 4x4, 2x8), -1 = the default (1x12). */
+ * 1x20, 4x4, 2x8), -1 = the default (1x16 in FP32, 1x12 in FP64). */
 int af_batch_create(int precision, int device, uint64_t arena_bytes, int variant,
                     af_batch** out);
 int af_batch_destroy(af_batch* b);
