@@ -584,6 +584,9 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
   const int strip = sx * p.nsy + sy;  // column-major: the special-cell order is R-independent
   int sp = p.spec_off[strip];
   const int sp_end = p.spec_off[strip + 1];
+  // Row of the strip's next special cell (INT_MAX: none left), loaded as soon
+  // as the previous one is consumed, so the row loop's test waits on nothing.
+  int next_row = sp < sp_end ? p.spec[sp].row : INT_MAX;
   // Rows to stream: j0-1 (H, DEM, Qx: the prologue) if j0 > 0, then j0..j1
   // (all four; row ny only exists for Qy).
   const int rfirst = j0 > 0 ? j0 - 1 : j0;
@@ -591,7 +594,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
   // Lanes 0..3 each copy one array (H, DEM, Qx, Qy) of row rfirst+k into
   // stage k; lane 0 also posts the expected byte count.  The prologue row
   // j0-1 has no Qy; row ny has only Qy.
-  const T* const src_of[4] = {H, Z, Qx, Qy};
+  const T* const my_src = lane == 0 ? H : lane == 1 ? Z : lane == 2 ? Qx : Qy;
   auto issue = [&](int k) {
     const int r = rfirst + k;
     const int slot = (kglob + k) % kStages;
@@ -600,8 +603,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
     if (lane == 0) mbar_expect_tx(&bar[slot], (uint32_t)((a_hi - a_lo) * kRowBytes));
     if (lane >= a_lo && lane < a_hi) {
       fence_proxy_async();
-      bulk_g2s(&ring[slot][lane][0], src_of[lane] + (long long)r * P + wcol, kRowBytes,
-               &bar[slot]);
+      bulk_g2s(&ring[slot][lane][0], my_src + (long long)r * P + wcol, kRowBytes, &bar[slot]);
     }
   };
   for (int k = 0; k < kStages && k < nload; k++) issue(k);
@@ -753,7 +755,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
       for (int k = 0; k < N; k++) hn[k] = h[k];
       const int sp_row = sp;
       // Point sources (src/main.cpp:245-262), before rain and the update.
-      while (sp < sp_end && p.spec[sp].row == j) {
+      while (next_row == j) {
         const SpecCell e = p.spec[sp];
         if (own) {
 #pragma unroll
@@ -765,6 +767,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
                                     p.dx, p.dA, t, dt);
         }
         sp++;
+        next_row = sp < sp_end ? p.spec[sp].row : INT_MAX;
       }
       update_cells(hn, qw, qe, qyn, qs, z, rain_on, rain_depth, dtT, dAT, dt_dA, ph.nodata);
       // Point depth BCs (src/kernels.cpp:259-277), after the update.
