@@ -757,14 +757,21 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
       // Point sources (src/main.cpp:245-262), before rain and the update.
       while (next_row == j) {
         const SpecCell e = p.spec[sp];
-        if (own) {
+        const int kc = e.col - cb;  // the lane's cell index of the special cell
+        if (own && kc >= 0 && kc < N) {
+          // One call site for the lane's N cells (selected, not indexed, so
+          // the cells stay in registers): keeps the row loop's code small.
+          T hv = hn[0];
+#pragma unroll
+          for (int k = 1; k < N; k++)
+            if (kc == k) hv = hn[k];
+          hv = apply_sources(hv, e.s0, e.s1,
+                             SeriesTable{p.src_type, p.src_value, p.src_off, p.src_times,
+                                         p.src_vals, p.src_sorted},
+                             p.dx, p.dA, t, dt);
 #pragma unroll
           for (int k = 0; k < N; k++)
-            if (cb + k == e.col)
-              hn[k] = apply_sources(hn[k], e.s0, e.s1,
-                                    SeriesTable{p.src_type, p.src_value, p.src_off, p.src_times,
-                                                p.src_vals, p.src_sorted},
-                                    p.dx, p.dA, t, dt);
+            if (kc == k) hn[k] = hv;
         }
         sp++;
         next_row = sp < sp_end ? p.spec[sp].row : INT_MAX;
