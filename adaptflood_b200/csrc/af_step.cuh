@@ -307,10 +307,14 @@ __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float
   const float2 dh = __fadd2_rn(dz, __fadd2_rn(h0, f2(-h1.x, -h1.y)));
   const float2 hfx = f2(dh.x >= 0.0f ? h0.x + fminf(0.0f, dz.x) : h1.x + fminf(0.0f, -dz.x),
                         dh.y >= 0.0f ? h0.y + fminf(0.0f, dz.y) : h1.y + fminf(0.0f, -dz.y));
-  const float2 hf = f2(fminf(fmaxf(hfx.x, 0.0f), ph.max_hflow),
-                       fminf(fmaxf(hfx.y, 0.0f), ph.max_hflow));
-  const bool wx = enable && z0.x != ph.nodata && z1.x != ph.nodata && hf.x > ph.depth_thresh;
-  const bool wy = enable && z0.y != ph.nodata && z1.y != ph.nodata && hf.y > ph.depth_thresh;
+  // The reference clamps the flow depth to [0, MaxHflow] and calls the face
+  // wet above DepthThresh; with DepthThresh >= 0 (fill_scalars makes the FP32
+  // threshold so) the clamp at 0 only matters for faces that are dry either
+  // way, whose values are discarded, so it is not applied.  The wet test is on
+  // the unclamped depth, so a NaN depth stays dry as in the reference.
+  const float2 hf = f2(fminf(hfx.x, ph.max_hflow), fminf(hfx.y, ph.max_hflow));
+  const bool wx = enable && z0.x != ph.nodata && z1.x != ph.nodata && hfx.x > ph.depth_thresh;
+  const bool wy = enable && z0.y != ph.nodata && z1.y != ph.nodata && hfx.y > ph.depth_thresh;
   any |= wx | wy;
   // In units of the stored Q (= Qold*dx): the reference's
   //   Q = (Qold - g*dt*hflow*Sf) / (1 + g*dt*n^2*|Qvect|/hflow^(10/3)) * dx
@@ -410,7 +414,7 @@ __device__ inline bool mbar_try_wait(uint64_t* b, uint32_t parity) {
 }
 // True once every lane has seen the phase complete; false after kWaitLimit polls.
 __device__ inline bool mbar_wait_warp(uint64_t* b, uint32_t parity) {
-  for (long long i = 0; i < kWaitLimit; i++) {
+  for (int i = 0; i < (int)kWaitLimit; i++) {
     const bool ok = mbar_try_wait(b, parity);
     if (__all_sync(0xffffffffu, ok)) return true;
   }
@@ -516,7 +520,9 @@ __device__ inline void fill_scalars(const StepParams& p, double t, double dt, do
   s.dt_dA = T(dt / p.dA);
   s.ph.dx = T(p.dx);
   s.ph.fn = T(p.fpn);
-  s.ph.depth_thresh = T(p.depth_thresh);
+  // FP32: at least 0 (the face law relies on it; a negative threshold makes
+  // the reference divide 0 by 0 on dry faces anyway).
+  s.ph.depth_thresh = sizeof(T) == 4 ? T(fmax(p.depth_thresh, 0.0)) : T(p.depth_thresh);
   s.ph.max_hflow = T(p.max_hflow);
   s.ph.nodata = T(p.nodata);
   s.ph.g = T(p.g);
