@@ -10,7 +10,11 @@ the batch keeps one R per size class (floor(log2(cells))).
 ``tune_rows`` measures, for each size class asked for, a batch of wet
 synthetic grids of that class large enough to fill the GPU, at each candidate
 R, and returns the fastest R per class (cell-updates/s, CUDA events on the
-batch's stream, after warm-up steps).  ``tune_variant`` picks the launch
+batch's stream, after warm-up steps; the better of two timings).  The
+load-adaptive strip height is off while it measures, so each candidate runs
+at its own height (with it on, the taller candidates would be cut down to the
+same height and the choice among them would be noise); a batch that uses
+the tuned heights keeps it on, to lower them when few scenarios remain.  ``tune_variant`` picks the launch
 shape (warps per block x resident blocks per SM) of the batch kernel the
 same way.  Results do not depend on R or the variant (bit for bit), only
 the speed does.
@@ -49,18 +53,21 @@ def _probe_case(cls: int, seed: int = 0) -> sc.Case:
     return c
 
 
-def _rate(batch: Batch, cases: Sequence[sc.Case], steps: int, warmup: int) -> float:
+def _rate(batch: Batch, cases: Sequence[sc.Case], steps: int, warmup: int,
+          repeats: int = 2) -> float:
     import torch
     slots = [batch.add(c) for c in cases]
     batch.run(max_steps=warmup)
     stream = torch.cuda.ExternalStream(batch.stream)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    batch.launch(max_steps=steps)
-    e1.record(stream)
-    batch.sync()
-    ms = e0.elapsed_time(e1)
+    ms = float("inf")
+    for _ in range(repeats):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        batch.launch(max_steps=steps)
+        e1.record(stream)
+        batch.sync()
+        ms = min(ms, e0.elapsed_time(e1))
     for s in slots:
         batch.remove(s)
     return sum(c.cells for c in cases) * steps / (ms / 1e3)
@@ -73,13 +80,14 @@ def _fill(cls: int, target_cells: int, cap: int = 256):
 
 
 def tune_rows(classes: Iterable[int], precision: str = "f32", device: int = 0,
-              rows: Sequence[int] = ROWS, target_cells: int = 1 << 25, steps: int = 12,
+              rows: Sequence[int] = ROWS, target_cells: int = 1 << 26, steps: int = 20,
               warmup: int = 3, variant: int = -1, arena_bytes: Optional[int] = None,
               scores_out: Optional[dict] = None) -> Dict[int, int]:
     """The fastest strip height per size class (`scores_out`, if given,
     receives the measured cell-updates/s per class and height)."""
     best: Dict[int, int] = {}
     with Batch(precision, device=device, variant=variant, arena_bytes=arena_bytes) as b:
+        b.set_balance(0)
         for cls in classes:
             cases = _fill(cls, target_cells)
             ny = cases[0].ny

@@ -188,3 +188,25 @@ def test_many_small_members(cuda):
             n, t, st, _ = _alone(cases[k], "f32")
             assert b.status(slots[k])[3] == n
             _assert_same(b.state(slots[k]), st)
+
+
+def test_tuned_rows_are_candidates_and_leave_results_unchanged(cuda):
+    """The autotuner returns one of its candidate heights per size class, with
+    a measured rate for every candidate; a batch run with the tuned heights
+    gives the same state as the scenario run alone."""
+    from adaptflood_b200.tune import tune_rows
+    scores = {}
+    rows = tune_rows([12, 14], "f32", rows=(4, 8, 16), target_cells=1 << 20, steps=4,
+                     warmup=1, arena_bytes=ARENA, scores_out=scores)
+    assert set(rows) == {12, 14}
+    for cls, r in rows.items():
+        assert r in (4, 8, 16)
+        assert set(scores[cls]) == {4, 8, 16}
+        assert all(v > 0 for v in scores[cls].values())
+    case = sc.small_case(90, 70, seed=41, rain=True, sim_time=200.0)
+    n, t, st, _ = _alone(case, "f32")
+    with Batch("f32", arena_bytes=ARENA, rows=rows) as b:
+        s = b.add(case)
+        b.run()
+        assert b.status(s)[3] == n
+        _assert_same(b.state(s), st)
