@@ -165,7 +165,7 @@ struct Batch {
   bool use_cond = false;
   bool in_flight = false;
   bool members_dirty = true;
-  int balance = 6;  // strips per warp the load-adaptive strip height aims at (0: off)
+  int balance = 4;  // strips per warp the load-adaptive strip height aims at (0: off)
   int hi_slot = 0;  // one past the highest slot ever used
   int rows[kClasses];
   std::vector<Slot> slots;

@@ -337,7 +337,7 @@ int af_batch_run(af_batch* b, int64_t max_steps, int64_t* batch_steps);
 /* Load-adaptive strip height: before each launch, the strip height of every
  * active member is the tuned height of its size class, lowered (powers of
  * two, at least 2 rows) until the active members give each warp of the
- * persistent grid about strips_per_warp strips.  0 turns it off (default 6).
+ * persistent grid about strips_per_warp strips.  0 turns it off (default 4).
  * Results do not depend on it. */
 int af_batch_set_balance(af_batch* b, int strips_per_warp);
 
