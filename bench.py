@@ -11,7 +11,8 @@ and the Hmax reduction that sets the next dt.
 Our arm times K steps of the fused kernel (one CUDA-graph launch, CUDA events
 on the simulation's stream) in FP32 (the headline `value`) and FP64, reports
 the HBM roofline of the step kernel, the end-to-end rate through the public
-C ABI with host buffers, and the reference's own CPU code timed on a bounded
+C ABI with host buffers (median of three runs, each reported), and the
+reference's own CPU code timed on a bounded
 sample of the same workload.  Two more legs (N = 1 only):
 
 * `ensemble`: 256 scenarios of 256^2..2048^2 cells, each with its own dt,
@@ -49,6 +50,7 @@ from adaptflood_b200 import scenarios as sc  # noqa: E402
 
 BYTES_PER_CELL = {"f32": 28, "f64": 56}  # read H, DEM, Qx, Qy; write H', Qx', Qy'
 T_START = 1800.0
+E2E_TRIALS = 3
 
 
 def parse():
@@ -445,8 +447,15 @@ def run_ours(args, rank: int, world: int):
     ach64 = BYTES_PER_CELL["f64"] * cells / (step_ms64 / 1e3) / 1e9
     tr32 = traffic_per_cell("k_step_f32")
     tr64 = traffic_per_cell("k_step_f64")
-    e2e_v, h2d, d2h, phases = ((0.0, 0, 0, {}) if args.no_e2e else
-                               time_e2e(case, forcing, "f32", args.steps, local))
+    # The median of E2E_TRIALS end-to-end runs: the host side of a shared GPU
+    # box (pinned-memory transfers, allocation) now and then stalls one run
+    # for hundreds of ms; every trial is reported.
+    trials = [] if args.no_e2e else [time_e2e(case, forcing, "f32", args.steps, local)
+                                     for _ in range(E2E_TRIALS)]
+    if trials:
+        e2e_v, h2d, d2h, phases = sorted(trials, key=lambda r: r[0])[len(trials) // 2]
+    else:
+        e2e_v, h2d, d2h, phases = 0.0, 0, 0, {}
     if dist is not None:
         t = torch.tensor([e2e_v], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MIN)
@@ -480,7 +489,9 @@ def run_ours(args, rank: int, world: int):
                     "d2h_bytes_per_step": int(d2h),
                     "path": "af_sim_create (DEM, start depth, forcing) from pinned host arrays, "
                             "K steps, af_sim_get_state of the depth field into pinned host memory",
-                    "phases": phases},
+                    "phases": phases,
+                    "trials": [t[0] for t in trials],
+                    "statistic": f"median of {len(trials)} runs"},
             "gpu_launches": args.steps + 1,
             "clocks": clk.summary(),
             "state_after": {"f32": info32, "f64": info64},
