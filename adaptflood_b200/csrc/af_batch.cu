@@ -244,21 +244,26 @@ static int build_graph(Batch& b) {
   cudaGraphNode_t cnode;
   AF_CUDA(cudaGraphAddNode(&cnode, b.graph, &b.begin_node, 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  // Body: the strips of every active scenario, then the fold.
+  // Body: kStepsPerIteration batch steps, each the strips of every active
+  // scenario, then the fold.
   void* sargs[] = {&b.bp};
   cudaKernelNodeParams ks{};
   ks.func = const_cast<void*>(b.kernel());
   ks.gridDim = b.grid;
   ks.blockDim = b.block;
   ks.kernelParams = sargs;
-  cudaGraphNode_t snode, fnode;
-  AF_CUDA(cudaGraphAddKernelNode(&snode, body, nullptr, 0, &ks));
   cudaKernelNodeParams kf{};
   kf.func = const_cast<void*>(b.fold_kernel());
   kf.gridDim = dim3(1);
   kf.blockDim = dim3(kFoldThreads);
   kf.kernelParams = sargs;
-  AF_CUDA(cudaGraphAddKernelNode(&fnode, body, &snode, 1, &kf));
+  cudaGraphNode_t prev = nullptr;
+  for (int k = 0; k < kStepsPerIteration; k++) {
+    cudaGraphNode_t snode, fnode;
+    AF_CUDA(cudaGraphAddKernelNode(&snode, body, prev ? &prev : nullptr, prev ? 1 : 0, &ks));
+    AF_CUDA(cudaGraphAddKernelNode(&fnode, body, &snode, 1, &kf));
+    prev = fnode;
+  }
   AF_CUDA(cudaGraphInstantiate(&b.exec, b.graph, 0));
   return AF_OK;
 }

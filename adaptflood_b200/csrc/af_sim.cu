@@ -447,14 +447,21 @@ static int build_graph(Sim& s) {
   AF_CUDA(cudaGraphAddNode(&cnode, s.graph, &s.begin_node, 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
 
+  // The loop body is kStepsPerIteration steps in a row: a step after the
+  // one that ended the loop finds the control block done and returns at
+  // once, and the loop test runs once per iteration instead of once per step.
   void* sargs[] = {&s.prm};
   cudaKernelNodeParams ks{};
   ks.func = const_cast<void*>(s.prec == AF_PREC_F64 ? step_kernel_f64(s.variant) : step_kernel_f32(s.variant));
   ks.gridDim = s.grid;
   ks.blockDim = s.block;
   ks.kernelParams = sargs;
-  cudaGraphNode_t snode;
-  AF_CUDA(cudaGraphAddKernelNode(&snode, body, nullptr, 0, &ks));
+  cudaGraphNode_t prev = nullptr;
+  for (int k = 0; k < kStepsPerIteration; k++) {
+    cudaGraphNode_t snode;
+    AF_CUDA(cudaGraphAddKernelNode(&snode, body, prev ? &prev : nullptr, prev ? 1 : 0, &ks));
+    prev = snode;
+  }
   AF_CUDA(cudaGraphInstantiate(&s.exec, s.graph, 0));
   return AF_OK;
 }

@@ -1031,6 +1031,10 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
 // max, and its volume partials are summed per strip in strip order.
 constexpr int kMaxSlots = 1024;
 constexpr int kFoldThreads = 1024;  // one block of the fold and begin kernels
+// Steps per iteration of a graph's while loop (single grid and batch): the
+// loop test runs once per iteration; steps after the one that ends the loop
+// return at once (the step and fold kernels check `done` first).
+constexpr int kStepsPerIteration = 4;
 
 // Per slot: the scenario's parameters and its coming step.  Copied whole
 // into shared memory by one bulk copy (16-byte size and alignment).
@@ -1174,6 +1178,7 @@ template <typename T>
 __global__ void __launch_bounds__(kFoldThreads) k_batch_fold(const BatchParams bp) {
   __shared__ double s_vol[kMaxSlots], s_area[kMaxSlots];
   BatchCtl* b = bp.bctl;
+  if (*(volatile int*)&b->done) return;  // the loop ended at an earlier step
   const BatchTab* tab = bp.tab;
   const int nact = tab->nact;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
