@@ -1010,7 +1010,8 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
 // ------------------------------------------------------------ batches
 // A batch advances many independent grids ("scenarios": each with its own
 // size, parameters, forcing, dt and time) by one step each per batch step.
-// A batch step is two kernels in the body of the graph's while loop:
+// A batch step is two kernels, and the body of the graph's while loop holds
+// kStepsPerIteration batch steps in a row:
 //   k_batch_step: the strips of every active scenario.  Units are numbered
 //     scenario after scenario (u0[a] = first unit of active scenario a); warp
 //     w of the persistent grid takes units w, w + W, ...; within a scenario,
