@@ -210,3 +210,18 @@ def test_tuned_rows_are_candidates_and_leave_results_unchanged(cuda):
         b.run()
         assert b.status(s)[3] == n
         _assert_same(b.state(s), st)
+
+
+def test_batch_step_limits_are_exact(cuda):
+    """A batch launch takes exactly the batch steps asked for, whatever the
+    number of steps per loop iteration."""
+    cases = _cases()
+    with Batch("f32", arena_bytes=ARENA) as b:
+        slots = [b.add(c) for c in cases[:3]]
+        total = 0
+        for n in (1, 2, 3, 5, 6):
+            b.launch(max_steps=n)
+            b.sync()
+            total += n
+            assert b.info()["batch_steps"] == total
+            assert all(b.status(s)[3] == total for s in slots)

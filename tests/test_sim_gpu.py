@@ -305,3 +305,16 @@ def test_checkpoint_restart_is_bit_identical(cuda, tmp_path, prec):
             d.restore(ck)
         with pytest.raises(AFError):
             d.restore(str(tmp_path / "missing.ckpt"))
+
+
+def test_step_limits_are_exact(cuda):
+    """The graph loop runs several steps per iteration; a launch still takes
+    exactly the steps asked for, and stops at its time limit mid-iteration."""
+    case, f, _ = load_golden("closed_rain_points")
+    with Simulation(case, "f32", forcing=f) as s:
+        for k, n in enumerate((1, 2, 3, 5, 7)):
+            assert s.run(1e30, max_steps=n) == n
+        assert s.status()[3] == 18
+        t = s.status()[0]
+        s.run(t + 1e-9, max_steps=100)  # one step ends the time limit
+        assert s.status()[3] == 19
