@@ -44,7 +44,7 @@ class OutputDesc(C.Structure):
         ("out_dir", C.c_char_p), ("save_int", C.c_double), ("voutput", C.c_int),
         ("async_style", C.c_int), ("xll", C.c_double), ("yll", C.c_double),
         ("n_stage", C.c_int), ("stage_idx", C.c_void_p), ("stage_names", C.c_void_p),
-        ("stage_int", C.c_double),
+        ("stage_int", C.c_double), ("output_format", C.c_int),
     ]
 
 

@@ -1,6 +1,7 @@
-// af_output.cpp -- ASC output (see af_output.h) and the af_write_asc entry
-// point.  Grids of 10^8 cells are written by formatting row blocks in
-// parallel into memory and writing the blocks in order.
+// af_output.cpp -- ASC and NetCDF output (see af_output.h) and the
+// af_write_asc entry point.  ASC grids of 10^8 cells are written by
+// formatting row blocks in parallel into memory and writing the blocks in
+// order.
 #include "af_output.h"
 
 #include <algorithm>
@@ -107,6 +108,151 @@ bool write_asc(const char* path, const double* values, int ncols, int nrows, dou
   }
   if (fclose(fp) != 0) ok = false;
   return ok;
+}
+
+// ------------------------------------------------------------ NetCDF
+namespace {
+
+// Big-endian encoders of the classic format's header and data.
+void put_u32(std::vector<unsigned char>& b, uint32_t v) {
+  for (int k = 3; k >= 0; k--) b.push_back((unsigned char)(v >> (8 * k)));
+}
+void put_u64(std::vector<unsigned char>& b, uint64_t v) {
+  for (int k = 7; k >= 0; k--) b.push_back((unsigned char)(v >> (8 * k)));
+}
+void put_f64(std::vector<unsigned char>& b, double x) {
+  uint64_t v;
+  std::memcpy(&v, &x, 8);
+  put_u64(b, v);
+}
+void put_f32(std::vector<unsigned char>& b, float x) {
+  uint32_t v;
+  std::memcpy(&v, &x, 4);
+  put_u32(b, v);
+}
+void pad4(std::vector<unsigned char>& b) {
+  while (b.size() % 4) b.push_back(0);
+}
+// A name: its length, then its bytes padded to 4.
+void put_name(std::vector<unsigned char>& b, const char* s) {
+  const uint32_t n = (uint32_t)std::strlen(s);
+  put_u32(b, n);
+  b.insert(b.end(), s, s + n);
+  pad4(b);
+}
+constexpr uint32_t kNcChar = 2, kNcFloat = 5, kNcDouble = 6;
+constexpr uint32_t kTagDimension = 10, kTagVariable = 11, kTagAttribute = 12;
+
+void put_text_att(std::vector<unsigned char>& b, const char* name, const char* text, int len) {
+  put_name(b, name);
+  put_u32(b, kNcChar);
+  put_u32(b, (uint32_t)len);
+  b.insert(b.end(), text, text + len);
+  pad4(b);
+}
+void put_double_att(std::vector<unsigned char>& b, const char* name, double v) {
+  put_name(b, name);
+  put_u32(b, kNcDouble);
+  put_u32(b, 1);
+  put_f64(b, v);
+}
+void put_float_att(std::vector<unsigned char>& b, const char* name, float v) {
+  put_name(b, name);
+  put_u32(b, kNcFloat);
+  put_u32(b, 1);
+  put_f32(b, v);
+}
+
+}  // namespace
+
+NcFile::~NcFile() {
+  if (fp_) fclose(fp_);
+}
+
+bool NcFile::open(const std::string& path, int nx, int ny, bool velocity, double xll, double yll,
+                  double cellsize, double nodata) {
+  ncells_ = (long long)nx * ny;
+  const long long vsize = ncells_ * 4;  // one record of H, Vx or Vy
+  if (nx <= 0 || ny <= 0 || vsize > 0xFFFFFFFCLL) return false;
+  velocity_ = velocity;
+  // The header is built twice: the variables' offsets depend on its size.
+  std::vector<unsigned char> h;
+  for (int pass = 0; pass < 2; pass++) {
+    const uint64_t hsize = h.size();
+    h.clear();
+    h.push_back('C'), h.push_back('D'), h.push_back('F'), h.push_back(2);
+    put_u32(h, 0);  // records so far
+    put_u32(h, kTagDimension);  // dimensions 0: time (the record dimension), 1: x, 2: y
+    put_u32(h, 3);
+    put_name(h, "time"), put_u32(h, 0);
+    put_name(h, "x"), put_u32(h, (uint32_t)nx);
+    put_name(h, "y"), put_u32(h, (uint32_t)ny);
+    put_u32(h, kTagAttribute);  // global attributes (src/async_output.cpp:47-49)
+    put_u32(h, 3);
+    put_double_att(h, "xllcorner", xll);
+    put_double_att(h, "yllcorner", yll);
+    put_double_att(h, "cellsize", cellsize);
+    put_u32(h, kTagVariable);
+    put_u32(h, velocity ? 4 : 2);
+    uint64_t begin = hsize;  // records start right after the header
+    // time(time): double, "seconds" (src/async_output.cpp:27-28)
+    put_name(h, "time");
+    put_u32(h, 1), put_u32(h, 0);
+    put_u32(h, kTagAttribute), put_u32(h, 1);
+    put_text_att(h, "units", "seconds", 7);
+    put_u32(h, kNcDouble), put_u32(h, 8), put_u64(h, begin);
+    begin += 8;
+    // H(time, y, x): float (src/async_output.cpp:30-35)
+    put_name(h, "H");
+    put_u32(h, 3), put_u32(h, 0), put_u32(h, 2), put_u32(h, 1);
+    put_u32(h, kTagAttribute), put_u32(h, 3);
+    put_text_att(h, "units", "m", 1);
+    put_text_att(h, "long_name", "water_depth", 11);
+    put_float_att(h, "_FillValue", (float)nodata);
+    put_u32(h, kNcFloat), put_u32(h, (uint32_t)vsize), put_u64(h, begin);
+    begin += vsize;
+    if (velocity) {  // src/async_output.cpp:37-45 (long_name lengths 16 as passed there)
+      const char* names[2] = {"Vx", "Vy"};
+      const char* longs[2] = {"x_direction_velocity", "y_direction_velocity"};
+      for (int v = 0; v < 2; v++) {
+        put_name(h, names[v]);
+        put_u32(h, 3), put_u32(h, 0), put_u32(h, 2), put_u32(h, 1);
+        put_u32(h, kTagAttribute), put_u32(h, 2);
+        put_text_att(h, "units", "m/s", 3);
+        put_text_att(h, "long_name", longs[v], 16);
+        put_u32(h, kNcFloat), put_u32(h, (uint32_t)vsize), put_u64(h, begin);
+        begin += vsize;
+      }
+    }
+  }
+  rec0_ = (long long)h.size();
+  recsize_ = 8 + vsize * (velocity ? 3 : 1);
+  nrec_ = 0;
+  fp_ = fopen(path.c_str(), "wb");
+  if (!fp_) return false;
+  return fwrite(h.data(), 1, h.size(), fp_) == h.size() && fflush(fp_) == 0;
+}
+
+bool NcFile::append(double time, const double* H, const double* Vx, const double* Vy) {
+  if (!fp_) return false;
+  buf_.clear();
+  buf_.reserve((size_t)recsize_);
+  put_f64(buf_, time);
+  const double* fields[3] = {H, Vx, Vy};
+  for (int f = 0; f < (velocity_ ? 3 : 1); f++)
+    for (long long i = 0; i < ncells_; i++)
+      put_f32(buf_, fields[f] ? (float)fields[f][i] : 0.0f);
+  std::vector<unsigned char> n;
+  put_u32(n, (uint32_t)(nrec_ + 1));
+  const long long off = rec0_ + (long long)nrec_ * recsize_;
+  if (fseeko(fp_, (off_t)off, SEEK_SET) != 0 || fwrite(buf_.data(), 1, buf_.size(), fp_) != buf_.size())
+    return false;
+  // The record count last, so a reader never sees a record before its data.
+  if (fflush(fp_) != 0 || fseeko(fp_, 4, SEEK_SET) != 0 || fwrite(n.data(), 1, 4, fp_) != 4 ||
+      fflush(fp_) != 0)
+    return false;
+  nrec_++;
+  return true;
 }
 
 Writer::Writer() : th_([this] { loop(); }) {}

@@ -32,6 +32,34 @@ enum AscStyle {
 bool write_asc(const char* path, const double* values, int ncols, int nrows, double xll,
                double yll, double cellsize, double nodata, int style, int threads);
 
+// The reference's NetCDF output (src/async_output.cpp:20-51, 109-138): one
+// file with dimensions time (unlimited), x = ncols, y = nrows; variables
+// time(time) double "seconds", H(time, y, x) float with units, long_name and
+// _FillValue = nodata, with velocity also Vx and Vy (their long_name cut to
+// the 16 characters the reference passes); global attributes xllcorner,
+// yllcorner and cellsize; one record per save, values rounded to float.
+// Written in NetCDF's classic container with 64-bit offsets (the published
+// classic format: big-endian header of dimension, attribute and variable
+// lists, then the records), which every NetCDF reader reads with the same
+// data model; the reference's NC_NETCDF4 flag selects the HDF5 container,
+// whose library is not available here.  The record count in the header is
+// rewritten after every record, so the file is complete after each one.
+class NcFile {
+ public:
+  ~NcFile();
+  // false on an I/O error or a grid whose one record of H exceeds 4 GiB - 4.
+  bool open(const std::string& path, int nx, int ny, bool velocity, double xll, double yll,
+            double cellsize, double nodata);
+  bool append(double time, const double* H, const double* Vx, const double* Vy);
+
+ private:
+  FILE* fp_ = nullptr;
+  long long ncells_ = 0, rec0_ = 0, recsize_ = 0;
+  int nrec_ = 0;
+  bool velocity_ = false;
+  std::vector<unsigned char> buf_;
+};
+
 // A single background thread that runs file-writing jobs in order.
 class Writer {
  public:

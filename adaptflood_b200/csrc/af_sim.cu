@@ -844,6 +844,11 @@ static int run_output(Sim& s, double sim_time, const af_output_desc& o, int64_t*
   const bool vel = o.voutput != 0;
   const int nf = vel ? 3 : 1;
   const int style = o.async_style ? kAscAsync : kAscSync;
+  if (o.output_format < 0 || o.output_format > 2) return AF_EINVAL;
+  // src/async_output.cpp:19, :144: the async writer writes NetCDF for formats
+  // 1 and 2 and the periodic ASC grids for 0 and 2; the synchronous one ASC.
+  const bool nc = o.async_style && o.output_format >= 1;
+  const bool asc_saves = !o.async_style || o.output_format != 1;
   const std::string dir(o.out_dir);
   DevBuf dsnap, didx, dval;
   AF_TRY(alloc_field(dsnap, cells * nf, 8));
@@ -891,6 +896,12 @@ static int run_output(Sim& s, double sim_time, const af_output_desc& o, int64_t*
   std::unique_ptr<FILE, int (*)(FILE*)> stage_guard(stage_fp, [](FILE* f) {
     return f ? fclose(f) : 0;
   });
+  std::unique_ptr<NcFile> ncf;  // declared before the writer, so it outlives its jobs
+  if (nc) {
+    ncf.reset(new NcFile);
+    if (!ncf->open(dir + "/output.nc", nx, ny, vel, o.xll, o.yll, s.c.dx, s.c.nodata))
+      return AF_EIO;
+  }
   Writer writer;
   double* snap = static_cast<double*>(dsnap.p);
 
@@ -905,8 +916,10 @@ static int run_output(Sim& s, double sim_time, const af_output_desc& o, int64_t*
     std::string tag;
     int style = 0;
     bool velocity = false;
+    bool periodic = false;  // a save of the loop (ASC and/or NetCDF), not the final grids
+    double t = 0.0;
   } pend;
-  auto snapshot = [&](const std::string& tag, int st, bool velocity) -> int {
+  auto snapshot = [&](const std::string& tag, int st, bool velocity, bool periodic) -> int {
     AF_TRY(read_ctl(s));
     const int par = s.pinned_ctl->parity;
     AF_CUDA(cudaStreamWaitEvent(s.st, R.ev_copy, 0));
@@ -927,6 +940,8 @@ static int run_output(Sim& s, double sim_time, const af_output_desc& o, int64_t*
     pend.tag = tag;
     pend.style = st;
     pend.velocity = velocity;
+    pend.periodic = periodic;
+    pend.t = s.pinned_ctl->t;
     return AF_OK;
   };
   auto ship = [&]() -> int {
@@ -942,18 +957,25 @@ static int run_output(Sim& s, double sim_time, const af_output_desc& o, int64_t*
     const double xll = o.xll, yll = o.yll, cs = s.c.dx, nd = s.c.nodata;
     const std::string tag = pend.tag;
     const int st = pend.style;
+    const bool asc = !pend.periodic || asc_saves;
+    NcFile* ncp = pend.periodic ? ncf.get() : nullptr;
+    const double ts = pend.t;
     cudaEvent_t ev = R.ev_copy;
-    writer.post([&writer, h, cells, dir, tag, st, velocity, nx, ny, xll, yll, cs, nd, ev] {
+    writer.post([&writer, h, cells, dir, tag, st, velocity, nx, ny, xll, yll, cs, nd, ev, asc,
+                 ncp, ts] {
       if (cudaEventSynchronize(ev) != cudaSuccess) {
         writer.fail();
         return;
       }
       const char* names[3] = {"H", "Vx", "Vy"};
-      for (int f = 0; f < (velocity ? 3 : 1); f++) {
+      for (int f = 0; asc && f < (velocity ? 3 : 1); f++) {
         const std::string path = dir + "/" + names[f] + "_" + tag + ".asc";
         if (!write_asc(path.c_str(), h + f * cells, nx, ny, xll, yll, cs, nd, st, 0))
           writer.fail();
       }
+      if (ncp && !ncp->append(ts, h, velocity ? h + cells : nullptr,
+                              velocity ? h + 2 * cells : nullptr))
+        writer.fail();
     });
     return AF_OK;
   };
@@ -967,7 +989,7 @@ static int run_output(Sim& s, double sim_time, const af_output_desc& o, int64_t*
   const long long step0 = s.pinned_ctl->step;
   double t = s.pinned_ctl->t;
   int save_num = 0;
-  AF_TRY(snapshot(tag_of(save_num++), style, vel && style == kAscAsync));  // src/main.cpp:206-225
+  AF_TRY(snapshot(tag_of(save_num++), style, vel && style == kAscAsync, true));  // src/main.cpp:206-225
   const double inf = 1e300;
   double next_save = o.save_int > 0.0 ? o.save_int : inf;  // src/main.cpp:199-201
   double next_stage = (nst > 0 && o.stage_int > 0.0) ? o.stage_int : inf;
@@ -1004,13 +1026,13 @@ static int run_output(Sim& s, double sim_time, const af_output_desc& o, int64_t*
       next_stage += o.stage_int;
     }
     if (t >= next_save) {  // src/main.cpp:325-363
-      AF_TRY(snapshot(tag_of(save_num++), style, vel && style == kAscAsync));
+      AF_TRY(snapshot(tag_of(save_num++), style, vel && style == kAscAsync, true));
       next_save += o.save_int;
     }
   }
   AF_TRY(ship());
   // Final state (src/main.cpp:376-388): always the synchronous writer's format.
-  AF_TRY(snapshot("final", kAscSync, vel));
+  AF_TRY(snapshot("final", kAscSync, vel, false));
   AF_TRY(ship());
   writer.drain();
   if (steps_out) *steps_out = s.pinned_ctl->step - step0;

@@ -168,16 +168,20 @@ class Simulation:
 
     def run_output(self, out_dir: str, sim_time: Optional[float] = None,
                    save_int: Optional[float] = None, voutput: bool = False,
-                   async_style: bool = False, stages=None, stage_int: float = 60.0) -> int:
+                   async_style: bool = False, stages=None, stage_int: float = 60.0,
+                   output_format: int = 0) -> int:
         """Runs to ``sim_time`` writing the reference's files into ``out_dir``
         (af_sim_run_output): H_%04d.asc every ``save_int``, H_final.asc, with
         ``voutput`` the velocity grids, and ``stage.csv`` for ``stages`` (a list
-        of (name, i, j) cells).  Returns the steps taken."""
+        of (name, i, j) cells); with ``async_style`` and ``output_format`` 1
+        (NetCDF) or 2 (both), the saves as records of output.nc.  Returns the
+        steps taken."""
         case = self.case
         o = _lib.OutputDesc()
         o.out_dir = os.fsencode(out_dir)
         o.save_int = float(case.save_int if save_int is None else save_int)
         o.voutput, o.async_style = int(voutput), int(async_style)
+        o.output_format = int(output_format)
         o.xll, o.yll = case.xll, case.yll
         keep = []
         if stages:

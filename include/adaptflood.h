@@ -242,8 +242,12 @@ int af_sim_restore(af_sim* s, const char* path);
  * stage_int, and H_final.asc (+ Vx_/Vy_final.asc with voutput) at the end.
  * async_style selects the header of the reference's async writer (xll/yll
  * "%.6f", NODATA "%.0f") rather than its synchronous one ("%.1f", "-9999").
- * Values are formatted exactly as printf("%.4f") does.  The GPU keeps stepping
- * while a save is copied out and written by a background thread. */
+ * Values are formatted exactly as printf("%.4f") does.  With async_style and
+ * output_format 1 or 2, each save is also a record of out_dir/output.nc
+ * (src/async_output.cpp:20-51, 109-138: time, H and with voutput Vx, Vy as
+ * float; NetCDF classic container with 64-bit offsets), and with format 1 the
+ * periodic ASC grids are not written.  The GPU keeps stepping while a save is
+ * copied out and written by a background thread. */
 typedef struct af_output_desc {
   const char* out_dir;   /* dirroot                                            */
   double save_int;       /* saveint; <= 0: no periodic saves                  */
@@ -254,6 +258,10 @@ typedef struct af_output_desc {
   const int* stage_idx;
   const char* const* stage_names;  /* NULL entries: "Stage<k>"                */
   double stage_int;      /* par key stageint                                  */
+  int output_format;     /* par key output_format: 0 ASC, 1 NetCDF, 2 both;    */
+                         /* as in the reference, NetCDF (output.nc, one record */
+                         /* per save) only with async_style, and the final     */
+                         /* grids are ASC whatever the format                  */
 } af_output_desc;
 
 /* Runs to sim_time with the outputs above; *steps (optional) = steps taken. */

@@ -96,3 +96,48 @@ def test_fp32_output_run_matches_fp64_within_tolerance(cuda, tmp_path):
     _, a = _read_asc(str(tmp_path / "f64" / "H_final.asc"))
     _, b = _read_asc(str(tmp_path / "f32" / "H_final.asc"))
     assert np.max(np.abs(np.array(a, float) - np.array(b, float))) <= 1e-3 + 1e-4
+
+
+@pytest.mark.parametrize("fmt", [1, 2])
+def test_netcdf_output(cuda, tmp_path, fmt):
+    """With the async writer and output_format 1 (NetCDF) or 2 (both), every
+    save is a record of output.nc with the reference's schema
+    (src/async_output.cpp:20-51: dimensions time/x/y, time in seconds, H, Vx,
+    Vy as float with their attributes, the georeference as global
+    attributes); the records hold the saved fields rounded to float, the last
+    one the final state.  Format 1 writes no periodic ASC grids, only the
+    final ones."""
+    from scipy.io import netcdf_file
+    case = _case()  # 300 s, saves every 60 s: the start and five more
+    out = str(tmp_path / "nc")
+    with Simulation(case, "f64") as s:
+        s.run_output(out, voutput=True, async_style=True, output_format=fmt)
+        t_end = s.status()[0]
+        H = s.depth()
+        Vx, Vy = s.velocity()
+    files = sorted(os.listdir(out))
+    assert "output.nc" in files and "H_final.asc" in files and "Vx_final.asc" in files
+    assert ("H_0003.asc" in files) == (fmt == 2)
+    with netcdf_file(os.path.join(out, "output.nc"), "r", mmap=False) as f:
+        assert f.version_byte == 2
+        assert f.dimensions["time"] is None
+        assert f.dimensions["x"] == case.nx and f.dimensions["y"] == case.ny
+        assert (f.xllcorner, f.yllcorner, f.cellsize) == (case.xll, case.yll, case.dx)
+        tv, hv, vx, vy = (f.variables[k] for k in ("time", "H", "Vx", "Vy"))
+        assert tv.units == b"seconds"
+        assert hv.units == b"m" and hv.long_name == b"water_depth"
+        assert hv._FillValue == np.float32(case.nodata)
+        assert vx.units == vy.units == b"m/s"
+        assert vx.long_name == b"x_direction_velo" and vy.long_name == b"y_direction_velo"
+        assert hv.dimensions == vx.dimensions == ("time", "y", "x")
+        times = tv[:].copy()
+        assert len(times) == 6 and times[0] == 0.0 and times[-1] == t_end
+        assert np.all(np.diff(times) > 0) and np.all(times[1:] >= 60.0 * np.arange(1, 6))
+        assert hv.shape == (6, case.ny, case.nx)
+        np.testing.assert_array_equal(hv[0], np.zeros((case.ny, case.nx), np.float32))
+        np.testing.assert_array_equal(hv[5], H.astype(np.float32))
+        np.testing.assert_array_equal(vx[5], Vx.astype(np.float32))
+        np.testing.assert_array_equal(vy[5], Vy.astype(np.float32))
+        if fmt == 2:
+            _, a = _read_asc(os.path.join(out, "H_0003.asc"))
+            assert np.max(np.abs(np.array(a, float) - hv[3].astype(float))) <= 5.01e-5 + 1e-6
