@@ -123,6 +123,7 @@ _SIGS = {
     "af_scenario_load": (_i, [C.c_char_p, _vp]),
     "af_scenario_free": (None, [_vp]),
     "af_scenario_get": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "af_scenario_output": (_i, [_vp, _vp]),
 }
 
 

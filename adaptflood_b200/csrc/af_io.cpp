@@ -355,7 +355,45 @@ struct af_scenario {
   std::vector<int> flow_idx, flow_type, flow_off, other_idx, other_type, other_off;
   std::vector<double> flow_value, flow_times, flow_vals, other_value, other_times, other_vals;
   std::vector<double> rain_times, rain_rates;
+  // outputs (af_scenario_output)
+  std::string out_dir;
+  double save_int = 0.0, stage_int = 0.0;
+  int voutput = 0, async_output = 1, output_format = 0;
+  std::vector<int> stage_idx;
+  std::vector<std::string> stage_names;
+  std::vector<const char*> stage_name_ptrs;
 };
+
+namespace {
+
+// src/io.cpp:50-85: stage points "x y [name]" in world coordinates, '#'
+// comments; grid cell by the truncating mapping of the BCI points; a missing
+// name is "Stage<n>".  The cell index the reference reads is gx + gy*ncols
+// when that lies in the grid (src/main.cpp:312-313), else the point prints NaN
+// (-1 here).  An unreadable file disables stage output, as there.
+void read_stage_file(const char* path, double xll, double yll, int ncols, int nrows, double cs,
+                     af_scenario& sc) {
+  std::ifstream f(path);
+  if (!f.is_open()) return;
+  const double tly = yll + nrows * cs;
+  std::string line;
+  while (std::getline(f, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream iss(line);
+    double x = 0.0, y = 0.0;
+    if (!(iss >> x >> y)) continue;
+    std::string name;
+    iss >> name;
+    if (name.empty()) name = "Stage" + std::to_string(sc.stage_names.size() + 1);
+    const long long gx = (long long)(int)((x - xll) / cs);
+    const long long gy = (long long)(int)((tly - y) / cs);
+    const long long idx = gx + gy * ncols;
+    sc.stage_idx.push_back(idx >= 0 && idx < (long long)ncols * nrows ? (int)idx : -1);
+    sc.stage_names.push_back(name);
+  }
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -405,6 +443,15 @@ int af_scenario_load(const char* parfile, af_scenario** out) {
   sc->geo[0] = xll;
   sc->geo[1] = yll;
   sc->geo[2] = cs;
+  sc->out_dir = p.output_dir;
+  sc->save_int = p.save_int;
+  sc->stage_int = p.stage_int;
+  sc->voutput = p.voutput;
+  sc->async_output = p.async_output;
+  sc->output_format = p.output_format;
+  if (!p.stage_file.empty())
+    read_stage_file(p.stage_file.c_str(), xll, yll, ncols, nrows, cs, *sc);
+  for (const std::string& n : sc->stage_names) sc->stage_name_ptrs.push_back(n.c_str());
 
   sc->flow_off.push_back(0);
   sc->other_off.push_back(0);
@@ -430,6 +477,23 @@ int af_scenario_load(const char* parfile, af_scenario** out) {
 }
 
 void af_scenario_free(af_scenario* sc) { delete sc; }
+
+int af_scenario_output(const af_scenario* sc, af_output_desc* o) {
+  if (!sc || !o) return AF_EINVAL;
+  *o = af_output_desc{};
+  o->out_dir = sc->out_dir.c_str();
+  o->save_int = sc->save_int;
+  o->voutput = sc->voutput;
+  o->async_style = sc->async_output;
+  o->xll = sc->geo[0];
+  o->yll = sc->geo[1];
+  o->n_stage = (int)sc->stage_idx.size();
+  o->stage_idx = sc->stage_idx.empty() ? nullptr : sc->stage_idx.data();
+  o->stage_names = sc->stage_name_ptrs.empty() ? nullptr : sc->stage_name_ptrs.data();
+  o->stage_int = sc->stage_int;
+  o->output_format = sc->output_format;
+  return AF_OK;
+}
 
 int af_scenario_get(const af_scenario* sc, af_case_desc* c, af_forcing_desc* f,
                     const double** dem, double* par, double* geo) {

@@ -265,3 +265,43 @@ def load_par(path: str) -> Tuple[sc.Case, fc.Forcing]:
         return case, forcing
     finally:
         lib.af_scenario_free(h)
+
+
+def par_outputs(path: str) -> dict:
+    """The outputs a ``.par`` case asks for, as the reference's CLI reads them
+    (af_scenario_output): out_dir, save_int, voutput, async_style,
+    output_format, stage_int and the stage points [(name, cell index or -1)]."""
+    lib = _lib.lib()
+    h = C.c_void_p()
+    _lib.check(lib.af_scenario_load(path.encode(), C.byref(h)), "af_scenario_load " + path)
+    try:
+        o = _lib.OutputDesc()
+        _lib.check(lib.af_scenario_output(h, C.byref(o)), "af_scenario_output")
+        names = C.cast(o.stage_names, C.POINTER(C.c_char_p)) if o.n_stage else None
+        idx = C.cast(o.stage_idx, C.POINTER(C.c_int)) if o.n_stage else None
+        return {"out_dir": o.out_dir.decode(), "save_int": o.save_int, "voutput": bool(o.voutput),
+                "async_style": bool(o.async_style), "output_format": o.output_format,
+                "stage_int": o.stage_int,
+                "stages": [(names[k].decode(), idx[k]) for k in range(o.n_stage)]}
+    finally:
+        lib.af_scenario_free(h)
+
+
+def run_par(path: str, precision: str = "f64", device: int = 0) -> int:
+    """Runs a ``.par`` case as the reference's CLI does (src/main.cpp): reads
+    its inputs, steps it to sim_time and writes the files it asks for
+    (af_sim_run_output with af_scenario_output).  Returns the steps taken."""
+    case, forcing = load_par(path)
+    lib = _lib.lib()
+    h = C.c_void_p()
+    _lib.check(lib.af_scenario_load(path.encode(), C.byref(h)), "af_scenario_load " + path)
+    try:
+        o = _lib.OutputDesc()
+        _lib.check(lib.af_scenario_output(h, C.byref(o)), "af_scenario_output")
+        with Simulation(case, precision, device=device, forcing=forcing) as s:
+            n = C.c_int64()
+            _lib.check(lib.af_sim_run_output(s.h, float(case.sim_time), C.byref(o), C.byref(n)),
+                       "af_sim_run_output")
+            return n.value
+    finally:
+        lib.af_scenario_free(h)

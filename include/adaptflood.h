@@ -386,6 +386,11 @@ void af_scenario_free(af_scenario* sc);
  * sim_time, save_int, mass_int; geo[0..2] = xll, yll, cellsize. */
 int af_scenario_get(const af_scenario* sc, af_case_desc* c, af_forcing_desc* f,
                     const double** dem, double* par, double* geo);
+/* The case's outputs as the reference's CLI writes them (src/io.cpp:9-47 keys
+ * dirroot, saveint, voutput, async_output, output_format, stageint; the stage
+ * points of stagefile read as src/io.cpp:50-85 does), for af_sim_run_output;
+ * the strings and arrays stay valid until af_scenario_free. */
+int af_scenario_output(const af_scenario* sc, af_output_desc* o);
 
 #ifdef __cplusplus
 }

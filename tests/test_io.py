@@ -183,3 +183,38 @@ def test_large_dem_parsed_in_parallel_equals_sequential_values(tmp_path):
         path.write_text(bad)
         with pytest.raises(_lib.AFError):
             load_par(par2)
+
+
+def test_par_outputs_and_stage_points(tmp_path):
+    """The output keys of a .par file and its stage points as the reference's
+    CLI reads them (src/io.cpp:9-85): '#' comments skipped, world
+    coordinates mapped by truncation, a missing name numbered "Stage<n>", a
+    point off the grid kept with no cell (NaN in stage.csv)."""
+    from adaptflood_b200.sim import par_outputs
+    c = sc.small_case(70, 50, seed=51, sim_time=300.0)
+    c.xll, c.yll = 1000.0, 2000.5
+    par = c.write(str(tmp_path / "in"), out_dir=str(tmp_path / "out"))
+    top = c.yll + c.ny * c.dx
+    with open(tmp_path / "st.txt", "w") as f:
+        f.write("# gauges\n")
+        f.write(f"{c.xll + 10.5 * c.dx} {top - 12.5 * c.dx} gauge_a\n")
+        f.write(f"{c.xll + 3.5 * c.dx} {top - 2.5 * c.dx}\n")
+        f.write(f"{c.xll + 5.5 * c.dx} {c.yll - 30 * c.dx} outside\n")
+    with open(par, "a") as f:
+        f.write(f"stagefile {tmp_path / 'st.txt'}\nstageint 30\noutput_format 2\nvoutput 1\n"
+                "async_output 1\nsaveint 120\n")
+    o = par_outputs(par)
+    assert o["out_dir"] == str(tmp_path / "out")
+    assert (o["save_int"], o["stage_int"], o["output_format"]) == (120.0, 30.0, 2)
+    assert o["voutput"] and o["async_style"]
+    assert o["stages"] == [("gauge_a", 10 + 12 * c.nx), ("Stage2", 3 + 2 * c.nx), ("outside", -1)]
+
+
+def test_par_without_stage_file_has_no_stage_points(tmp_path):
+    from adaptflood_b200.sim import par_outputs
+    c = sc.small_case(20, 10, seed=3, sim_time=60.0)
+    par = c.write(str(tmp_path / "in"), out_dir=str(tmp_path / "out"))
+    with open(par, "a") as f:
+        f.write(f"stagefile {tmp_path / 'missing.txt'}\n")
+    o = par_outputs(par)
+    assert o["stages"] == [] and o["output_format"] == 0 and not o["async_style"]

@@ -62,6 +62,30 @@ def test_outputs_match_reference_cli(cuda, tmp_path, voutput, async_out):
     ours = str(tmp_path / "ours")
     with Simulation(case, "f64") as s:
         s.run_output(ours, voutput=voutput, async_style=async_out, stages=STAGES, stage_int=30.0)
+    _compare_with_reference(case, ref_dir, ours)
+
+
+def test_par_file_run_matches_reference_cli(cuda, tmp_path):
+    """The same .par file run by run_par (inputs, outputs and stage points all
+    read by this library, af_scenario_output) and by the reference's CLI
+    gives the same files."""
+    if not os.path.exists(orc.REF_CLI):
+        pytest.skip("reference CLI not built")
+    from adaptflood_b200.sim import run_par
+    case = _case()
+    ref_dir = _run_reference(case, str(tmp_path), True, True)
+    par = os.path.join(str(tmp_path), "ref_in", "case.par")
+    ours = str(tmp_path / "ours")
+    mine = os.path.join(str(tmp_path), "mine.par")
+    with open(par) as f, open(mine, "w") as g:
+        for line in f:
+            g.write(f"dirroot {ours}\n" if line.startswith("dirroot") else line)
+    os.makedirs(ours, exist_ok=True)
+    run_par(mine, "f64")
+    _compare_with_reference(case, ref_dir, ours)
+
+
+def _compare_with_reference(case, ref_dir, ours):
     ref_files = sorted(f for f in os.listdir(ref_dir) if f.endswith((".asc", ".csv")))
     our_files = sorted(os.listdir(ours))
     assert our_files == ref_files
