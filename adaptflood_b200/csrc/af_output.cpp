@@ -235,18 +235,33 @@ bool NcFile::open(const std::string& path, int nx, int ny, bool velocity, double
 
 bool NcFile::append(double time, const double* H, const double* Vx, const double* Vy) {
   if (!fp_) return false;
+  const long long off = rec0_ + (long long)nrec_ * recsize_;
+  if (fseeko(fp_, (off_t)off, SEEK_SET) != 0) return false;
   buf_.clear();
-  buf_.reserve((size_t)recsize_);
   put_f64(buf_, time);
+  if (fwrite(buf_.data(), 1, buf_.size(), fp_) != buf_.size()) return false;
+  // The fields in chunks of 1 Mi values, converted to big-endian float.
+  constexpr long long kChunk = 1 << 20;
   const double* fields[3] = {H, Vx, Vy};
-  for (int f = 0; f < (velocity_ ? 3 : 1); f++)
-    for (long long i = 0; i < ncells_; i++)
-      put_f32(buf_, fields[f] ? (float)fields[f][i] : 0.0f);
+  for (int f = 0; f < (velocity_ ? 3 : 1); f++) {
+    for (long long i0 = 0; i0 < ncells_; i0 += kChunk) {
+      const long long i1 = std::min(ncells_, i0 + kChunk);
+      buf_.resize((size_t)(i1 - i0) * 4);
+      unsigned char* o = buf_.data();
+      for (long long i = i0; i < i1; i++, o += 4) {
+        const float x = fields[f] ? (float)fields[f][i] : 0.0f;
+        uint32_t u;
+        std::memcpy(&u, &x, 4);
+#if __BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__
+        u = __builtin_bswap32(u);
+#endif
+        std::memcpy(o, &u, 4);
+      }
+      if (fwrite(buf_.data(), 1, buf_.size(), fp_) != buf_.size()) return false;
+    }
+  }
   std::vector<unsigned char> n;
   put_u32(n, (uint32_t)(nrec_ + 1));
-  const long long off = rec0_ + (long long)nrec_ * recsize_;
-  if (fseeko(fp_, (off_t)off, SEEK_SET) != 0 || fwrite(buf_.data(), 1, buf_.size(), fp_) != buf_.size())
-    return false;
   // The record count last, so a reader never sees a record before its data.
   if (fflush(fp_) != 0 || fseeko(fp_, 4, SEEK_SET) != 0 || fwrite(n.data(), 1, 4, fp_) != 4 ||
       fflush(fp_) != 0)
