@@ -36,9 +36,11 @@ UNITS = [
     ("af_step_f32.cu", FAST),
     ("af_sim.cu", EXACT),
     ("af_batch.cu", EXACT),
+    ("af_xfer.cu", EXACT),
 ]
 HOST_UNITS = ["af_io.cpp", "af_arena.cpp", "af_output.cpp"]
-HEADERS = ["af_common.cuh", "af_step.cuh", "af_simcore.cuh", "af_arena.h", "af_output.h"]
+HEADERS = ["af_common.cuh", "af_step.cuh", "af_simcore.cuh", "af_arena.h", "af_output.h",
+           "af_xfer.h"]
 
 
 def _newer(target: str, deps) -> bool:

@@ -35,6 +35,7 @@
 
 #include "af_arena.h"
 #include "af_simcore.cuh"
+#include "af_xfer.h"
 
 namespace af {
 
@@ -344,15 +345,13 @@ template <typename T>
 static int put_padded(Batch& b, char* dst, const double* src, int rows, int width, int P) {
   T* d = reinterpret_cast<T*>(dst) + kGuard;
   if (sizeof(T) == 8) {
-    AF_CUDA(cudaMemcpy2DAsync(d, (size_t)P * 8, src, (size_t)width * 8, (size_t)width * 8, rows,
-                              cudaMemcpyHostToDevice, b.cst));
+    AF_CUDA(copy2d_h2d(d, (size_t)P * 8, src, (size_t)width * 8, (size_t)width * 8, rows, b.cst));
   } else {
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>(rows, kStageBytes / (8 * (size_t)width)));
     for (int j = 0; j < rows; j += chunk) {
       const int n = std::min(chunk, rows - j);
-      AF_CUDA(cudaMemcpy2DAsync(b.stage, (size_t)width * 8, src + (size_t)j * width,
-                                (size_t)width * 8, (size_t)width * 8, n, cudaMemcpyHostToDevice,
-                                b.cst));
+      AF_CUDA(copy2d_h2d(b.stage, (size_t)width * 8, src + (size_t)j * width, (size_t)width * 8,
+                         (size_t)width * 8, n, b.cst));
       k_pad_from_f64<<<grid_for((long long)n * width, 256, 8), 256, 0, b.cst>>>(
           b.stage, n, width, reinterpret_cast<float*>(d) + (size_t)j * P, P);
       AF_CUDA(cudaGetLastError());
@@ -642,8 +641,7 @@ template <typename T>
 static int get_field(Batch& b, const char* src, int rows, int width, int P, double* dst,
                      size_t hpitch) {
   if (sizeof(T) == 8) {
-    AF_CUDA(cudaMemcpy2DAsync(dst, hpitch * 8, src, (size_t)P * 8, (size_t)width * 8, rows,
-                              cudaMemcpyDeviceToHost, b.cst));
+    AF_CUDA(copy2d_d2h(dst, hpitch * 8, src, (size_t)P * 8, (size_t)width * 8, rows, b.cst));
   } else {
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>(rows, kStageBytes / (8 * (size_t)width)));
     for (int j = 0; j < rows; j += chunk) {
@@ -651,8 +649,8 @@ static int get_field(Batch& b, const char* src, int rows, int width, int P, doub
       k_dense_to_f64<<<grid_for((long long)n * width, 256, 8), 256, 0, b.cst>>>(
           reinterpret_cast<const float*>(src) + (size_t)j * P, P, n, width, b.stage);
       AF_CUDA(cudaGetLastError());
-      AF_CUDA(cudaMemcpy2DAsync(dst + (size_t)j * hpitch, hpitch * 8, b.stage, (size_t)width * 8,
-                                (size_t)width * 8, n, cudaMemcpyDeviceToHost, b.cst));
+      AF_CUDA(copy2d_d2h(dst + (size_t)j * hpitch, hpitch * 8, b.stage, (size_t)width * 8,
+                         (size_t)width * 8, n, b.cst));
     }
   }
   AF_CUDA(cudaStreamSynchronize(b.cst));

@@ -18,6 +18,7 @@
 
 #include "af_output.h"
 #include "af_simcore.cuh"
+#include "af_xfer.h"
 
 namespace af {
 
@@ -339,8 +340,7 @@ static int alloc_field(DevBuf& b, size_t elems, int esize) {
 static int put_field(Sim& s, DevBuf& b, const double* src, int rows, int width, size_t hpitch) {
   char* dst = static_cast<char*>(b.p) + (size_t)kGuard * s.esize;
   if (s.prec == AF_PREC_F64) {
-    AF_CUDA(cudaMemcpy2DAsync(dst, (size_t)s.P * 8, src, hpitch * 8, (size_t)width * 8, rows,
-                              cudaMemcpyHostToDevice, s.st));
+    AF_CUDA(copy2d_h2d(dst, (size_t)s.P * 8, src, hpitch * 8, (size_t)width * 8, rows, s.st));
     AF_CUDA(cudaStreamSynchronize(s.st));
     return AF_OK;
   }
@@ -349,8 +349,8 @@ static int put_field(Sim& s, DevBuf& b, const double* src, int rows, int width, 
   AF_TRY(alloc_field(stage, (size_t)chunk * width, 8));
   for (int j = 0; j < rows; j += chunk) {
     const int n = std::min(chunk, rows - j);
-    AF_CUDA(cudaMemcpy2DAsync(stage.p, (size_t)width * 8, src + (size_t)j * hpitch, hpitch * 8,
-                              (size_t)width * 8, n, cudaMemcpyHostToDevice, s.st));
+    AF_CUDA(copy2d_h2d(stage.p, (size_t)width * 8, src + (size_t)j * hpitch, hpitch * 8,
+                       (size_t)width * 8, n, s.st));
     k_pad_from_f64<<<grid_for((long long)n * width, 256, 8), 256, 0, s.st>>>(
         static_cast<const double*>(stage.p), n, width,
         reinterpret_cast<float*>(dst) + (size_t)j * s.P, s.P);
@@ -363,8 +363,7 @@ static int put_field(Sim& s, DevBuf& b, const double* src, int rows, int width, 
 static int get_field(Sim& s, DevBuf& b, double* dst, int rows, int width, size_t hpitch) {
   const char* src = static_cast<const char*>(b.p) + (size_t)kGuard * s.esize;
   if (s.prec == AF_PREC_F64) {
-    AF_CUDA(cudaMemcpy2DAsync(dst, hpitch * 8, src, (size_t)s.P * 8, (size_t)width * 8, rows,
-                              cudaMemcpyDeviceToHost, s.st));
+    AF_CUDA(copy2d_d2h(dst, hpitch * 8, src, (size_t)s.P * 8, (size_t)width * 8, rows, s.st));
     AF_CUDA(cudaStreamSynchronize(s.st));
     return AF_OK;
   }
@@ -377,8 +376,8 @@ static int get_field(Sim& s, DevBuf& b, double* dst, int rows, int width, size_t
         reinterpret_cast<const float*>(src) + (size_t)j * s.P, s.P, n, width,
         static_cast<double*>(stage.p));
     AF_CUDA(cudaGetLastError());
-    AF_CUDA(cudaMemcpy2DAsync(dst + (size_t)j * hpitch, hpitch * 8, stage.p, (size_t)width * 8,
-                              (size_t)width * 8, n, cudaMemcpyDeviceToHost, s.st));
+    AF_CUDA(copy2d_d2h(dst + (size_t)j * hpitch, hpitch * 8, stage.p, (size_t)width * 8,
+                       (size_t)width * 8, n, s.st));
   }
   AF_CUDA(cudaStreamSynchronize(s.st));
   return AF_OK;
@@ -1050,11 +1049,9 @@ static int field_io(Sim& s, DevBuf& b, std::vector<char>& host, int rows, int wi
   char* dev = static_cast<char*>(b.p) + (size_t)kGuard * s.esize;
   const size_t w = (size_t)width * s.esize;
   if (put)
-    AF_CUDA(cudaMemcpy2DAsync(dev, (size_t)s.P * s.esize, host.data(), w, w, rows,
-                              cudaMemcpyHostToDevice, s.st));
+    AF_CUDA(copy2d_h2d(dev, (size_t)s.P * s.esize, host.data(), w, w, rows, s.st));
   else
-    AF_CUDA(cudaMemcpy2DAsync(host.data(), w, dev, (size_t)s.P * s.esize, w, rows,
-                              cudaMemcpyDeviceToHost, s.st));
+    AF_CUDA(copy2d_d2h(host.data(), w, dev, (size_t)s.P * s.esize, w, rows, s.st));
   AF_CUDA(cudaStreamSynchronize(s.st));
   return AF_OK;
 }
