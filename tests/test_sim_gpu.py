@@ -318,3 +318,23 @@ def test_step_limits_are_exact(cuda):
         t = s.status()[0]
         s.run(t + 1e-9, max_steps=100)  # one step ends the time limit
         assert s.status()[3] == 19
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_large_fields_round_trip_from_pageable_memory(cuda, prec):
+    """Fields of several pinned-buffer loads each (40 MB as FP64) go in and
+    come back through the library's staged copies unchanged (FP32: rounded
+    to float once)."""
+    nx, ny = 2500, 2000
+    case = sc.small_case(nx, ny, seed=61, sim_time=60.0)
+    rng = np.random.default_rng(61)
+    H = rng.uniform(0.0, 3.0, (ny, nx))
+    Qx = rng.normal(0.0, 1.0, (ny + 1, nx + 1))  # reference layout: (nx+1)*(ny+1) faces
+    Qy = rng.normal(0.0, 1.0, (ny + 1, nx + 1))
+    with Simulation(case, prec) as s:
+        s.set_state(H, Qx, Qy, 12.5)
+        st = s.state()
+    cast = (lambda a: a) if prec == "f64" else (lambda a: a.astype(np.float32).astype(np.float64))
+    np.testing.assert_array_equal(st["H"], cast(H))
+    np.testing.assert_array_equal(st["Qx"][:ny, :], cast(Qx[:ny, :]))
+    np.testing.assert_array_equal(st["Qy"][:, :nx], cast(Qy[:, :nx]))
