@@ -18,6 +18,7 @@ namespace af {
 namespace {
 
 constexpr size_t kBufBytes = 16u << 20;  // each of the two pinned buffers
+constexpr size_t kMinStaged = 1u << 20;  // smaller copies: the driver's own path is as quick
 
 // Worker threads that run the pieces of one host-side copy; the calling
 // thread takes pieces too.
@@ -166,7 +167,7 @@ cudaError_t copy2d_h2d(void* dst, size_t dpitch, const void* src, size_t spitch,
                        size_t rows, cudaStream_t st) {
   if (rows == 0 || width == 0) return cudaSuccess;
   Staging& S = staging();
-  if (width > kBufBytes || !pageable(src))
+  if (width > kBufBytes || width * rows < kMinStaged || !pageable(src))
     return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyHostToDevice, st);
   std::lock_guard<std::mutex> g(S.mu);
   if (!ready(S))
@@ -202,7 +203,7 @@ cudaError_t copy2d_d2h(void* dst, size_t dpitch, const void* src, size_t spitch,
                        size_t rows, cudaStream_t st) {
   if (rows == 0 || width == 0) return cudaSuccess;
   Staging& S = staging();
-  if (width > kBufBytes || !pageable(dst))
+  if (width > kBufBytes || width * rows < kMinStaged || !pageable(dst))
     return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyDeviceToHost, st);
   std::lock_guard<std::mutex> g(S.mu);
   if (!ready(S))

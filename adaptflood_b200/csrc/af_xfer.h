@@ -2,14 +2,14 @@
 // in or reads back) at the link's rate whether or not the host memory is
 // pinned.
 //
-// Pinned (page-locked) host memory is copied by DMA straight away
-// (cudaMemcpy2DAsync).  Pageable memory, which the driver would copy through
-// its own small staging buffers at a fraction of the link's rate, goes
-// through two 16 MB pinned buffers of this library instead: host threads
-// fill one (or drain it) while the DMA of the other runs.  Such a copy
-// returns when the host side is done with the caller's memory (for a copy to
-// the device: when the data has left this library's buffers too).  Copies
-// through the buffers run one at a time per process.
+// Pinned (page-locked) host memory, and any copy under 1 MB, is copied by
+// cudaMemcpy2DAsync straight away.  Larger copies of pageable memory, which
+// the driver would move through its own small staging buffers at a fraction
+// of the link's rate, go through two 16 MB pinned buffers of this library
+// instead: host threads fill one (or drain it) while the DMA of the other
+// runs.  Such a copy returns when the host side is done with the caller's
+// memory (for a copy to the device: when the data has left this library's
+// buffers too).  Copies through the buffers run one at a time per process.
 #pragma once
 
 #include <cuda_runtime.h>
