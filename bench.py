@@ -38,6 +38,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -108,7 +109,10 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # raw samples (the summary goes into the JSON line); BENCH_CLOCKS_DIR
+        # keeps them somewhere of the caller's choosing
+        d = os.environ.get("BENCH_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(d, f"clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
