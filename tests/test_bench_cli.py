@@ -1,5 +1,5 @@
 """bench.py imports without a device, parses its defaults, and defines every
-leg its runner calls (a leg that went missing would only fail on a GPU box)."""
+leg its runner calls (a leg that went missing would otherwise only fail on a GPU)."""
 import ast
 import os
 import sys
