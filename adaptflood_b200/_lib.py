@@ -96,6 +96,9 @@ _SIGS = {
     "af_sim_checkpoint": (_i, [_vp, C.c_char_p]),
     "af_sim_restore": (_i, [_vp, C.c_char_p]),
     "af_write_asc": (_i, [C.c_char_p, _vp, _i, _i, _d, _d, _d, _d, _i]),
+    "af_netcdf_create": (_i, [C.c_char_p, _i, _i, _i, _d, _d, _d, _d, _vp]),
+    "af_netcdf_append": (_i, [_vp, _d, _vp, _vp, _vp]),
+    "af_netcdf_close": (_i, [_vp]),
     "af_batch_create": (_i, [_i, _i, _u64, _i, _vp]),
     "af_batch_destroy": (_i, [_vp]),
     "af_batch_size_class": (_i, [_i, _i]),

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <new>
 
 #include "adaptflood.h"
 
@@ -318,6 +319,38 @@ void Writer::loop() {
 }
 
 }  // namespace af
+
+struct af_netcdf {
+  af::NcFile f;
+  bool velocity = false;
+};
+
+extern "C" int af_netcdf_create(const char* path, int ncols, int nrows, int voutput, double xll,
+                                double yll, double cellsize, double nodata, af_netcdf** out) {
+  if (!path || !out || ncols <= 0 || nrows <= 0) return AF_EINVAL;
+  if ((long long)ncols * nrows * 4 > 0xFFFFFFFCLL) return AF_ERANGE;
+  af_netcdf* h = new (std::nothrow) af_netcdf();
+  if (!h) return AF_ENOMEM;
+  h->velocity = voutput != 0;
+  if (!h->f.open(path, ncols, nrows, h->velocity, xll, yll, cellsize, nodata)) {
+    delete h;
+    return AF_EIO;
+  }
+  *out = h;
+  return AF_OK;
+}
+
+extern "C" int af_netcdf_append(af_netcdf* f, double time, const double* H, const double* Vx,
+                                const double* Vy) {
+  if (!f || !H || (f->velocity && (!Vx || !Vy))) return AF_EINVAL;
+  return f->f.append(time, H, f->velocity ? Vx : nullptr, f->velocity ? Vy : nullptr) ? AF_OK
+                                                                                     : AF_EIO;
+}
+
+extern "C" int af_netcdf_close(af_netcdf* f) {
+  delete f;
+  return AF_OK;
+}
 
 extern "C" int af_write_asc(const char* path, const double* values, int ncols, int nrows,
                             double xll, double yll, double cellsize, double nodata, int style) {

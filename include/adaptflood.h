@@ -273,6 +273,21 @@ int af_sim_run_output(af_sim* s, double sim_time, const af_output_desc* o, int64
 int af_write_asc(const char* path, const double* values, int ncols, int nrows, double xll,
                  double yll, double cellsize, double nodata, int style);
 
+/* The NetCDF file of the reference's async writer (src/async_output.cpp:20-51,
+ * 109-138) from host arrays, for a caller that runs its own loop: dimensions
+ * time (unlimited), x, y; time(time) double; H(time, y, x) float (with voutput
+ * Vx and Vy too) with the reference's attributes; one record per append,
+ * values rounded to float; NetCDF's classic container with 64-bit offsets.
+ * The record count in the file is updated after every record.  AF_ERANGE for
+ * a grid whose one record of a field exceeds 4 GiB - 4 bytes. */
+typedef struct af_netcdf af_netcdf;
+int af_netcdf_create(const char* path, int ncols, int nrows, int voutput, double xll, double yll,
+                     double cellsize, double nodata, af_netcdf** out);
+/* Vx and Vy are read only when the file was created with voutput. */
+int af_netcdf_append(af_netcdf* f, double time, const double* H, const double* Vx,
+                     const double* Vy);
+int af_netcdf_close(af_netcdf* f);
+
 /* ======================================================= 3. batch layer == */
 
 /* No counterpart in the reference, which runs one grid per process: a batch
