@@ -131,12 +131,13 @@ bool ready(Staging& s) {
   return s.buf[0] != nullptr;
 }
 
-// Pageable host memory: the driver cannot DMA it directly.
+// Pageable host memory: the driver cannot DMA it directly.  A pointer CUDA
+// cannot classify goes to cudaMemcpy2DAsync, which reports the error.
 bool pageable(const void* p) {
   cudaPointerAttributes a{};
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
-    return true;
+    return false;
   }
   return a.type == cudaMemoryTypeUnregistered;
 }

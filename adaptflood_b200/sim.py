@@ -219,52 +219,62 @@ class Simulation:
 
 def load_par(path: str) -> Tuple[sc.Case, fc.Forcing]:
     """Parses a ``.par`` case with the library's reader (reference rules)."""
-    lib = _lib.lib()
-    h = C.c_void_p()
-    _lib.check(lib.af_scenario_load(path.encode(), C.byref(h)), "af_scenario_load " + path)
+    h = _open_par(path)
     try:
-        d = _lib.CaseDesc()
-        f = _lib.ForcingDesc()
-        dem_p = C.POINTER(C.c_double)()
-        par = np.zeros(3)
-        geo = np.zeros(3)
-        _lib.check(lib.af_scenario_get(h, C.byref(d), C.byref(f), C.byref(dem_p), _p(par), _p(geo)),
-                   "af_scenario_get")
-        nx, ny = d.nx, d.ny
-        dem = np.ctypeslib.as_array(dem_p, shape=(ny * nx,)).copy().reshape(ny, nx) if nx * ny else \
-            np.zeros((ny, nx))
-
-        def arr(ptr, n, dt):
-            if n == 0 or not ptr:
-                return np.zeros(0, dtype=dt)
-            ct = C.c_int if dt == np.int32 else C.c_double
-            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(n,)).copy()
-
-        fo = arr(f.flow_off, f.n_flow + 1, np.int32)
-        oo = arr(f.other_off, f.n_other + 1, np.int32)
-        forcing = fc.Forcing(
-            flow_idx=arr(f.flow_idx, f.n_flow, np.int32), flow_type=arr(f.flow_type, f.n_flow, np.int32),
-            flow_value=arr(f.flow_value, f.n_flow, np.float64), flow_off=fo,
-            flow_times=arr(f.flow_times, int(fo[-1]) if len(fo) else 0, np.float64),
-            flow_vals=arr(f.flow_vals, int(fo[-1]) if len(fo) else 0, np.float64),
-            other_idx=arr(f.other_idx, f.n_other, np.int32),
-            other_type=arr(f.other_type, f.n_other, np.int32),
-            other_value=arr(f.other_value, f.n_other, np.float64), other_off=oo,
-            other_times=arr(f.other_times, int(oo[-1]) if len(oo) else 0, np.float64),
-            other_vals=arr(f.other_vals, int(oo[-1]) if len(oo) else 0, np.float64),
-            rain_times=arr(f.rain_times, f.n_rain, np.float64),
-            rain_rates=arr(f.rain_rates, f.n_rain, np.float64))
-        case = sc.Case(nx, ny, d.dx, dem, xll=float(geo[0]), yll=float(geo[1]), nodata=d.nodata,
-                       sim_time=float(par[0]), save_int=float(par[1]), mass_int=float(par[2]),
-                       init_tstep=d.init_tstep, cfl=d.cfl, fpn=d.fpn, depth_thresh=d.depth_thresh,
-                       west_free=bool(d.west_free), east_free=bool(d.east_free),
-                       north_free=bool(d.north_free), south_free=bool(d.south_free),
-                       name=path)
-        if forcing.n_rain:
-            case.rain_times, case.rain_rates = forcing.rain_times, forcing.rain_rates
-        return case, forcing
+        return _case_of(h, path)
     finally:
-        lib.af_scenario_free(h)
+        _lib.lib().af_scenario_free(h)
+
+
+def _open_par(path: str) -> C.c_void_p:
+    h = C.c_void_p()
+    _lib.check(_lib.lib().af_scenario_load(path.encode(), C.byref(h)), "af_scenario_load " + path)
+    return h
+
+
+def _case_of(h: C.c_void_p, path: str) -> Tuple[sc.Case, fc.Forcing]:
+    """The case and forcing of an open scenario (af_scenario_get)."""
+    lib = _lib.lib()
+    d = _lib.CaseDesc()
+    f = _lib.ForcingDesc()
+    dem_p = C.POINTER(C.c_double)()
+    par = np.zeros(3)
+    geo = np.zeros(3)
+    _lib.check(lib.af_scenario_get(h, C.byref(d), C.byref(f), C.byref(dem_p), _p(par), _p(geo)),
+               "af_scenario_get")
+    nx, ny = d.nx, d.ny
+    dem = np.ctypeslib.as_array(dem_p, shape=(ny * nx,)).copy().reshape(ny, nx) if nx * ny else \
+        np.zeros((ny, nx))
+
+    def arr(ptr, n, dt):
+        if n == 0 or not ptr:
+            return np.zeros(0, dtype=dt)
+        ct = C.c_int if dt == np.int32 else C.c_double
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(n,)).copy()
+
+    fo = arr(f.flow_off, f.n_flow + 1, np.int32)
+    oo = arr(f.other_off, f.n_other + 1, np.int32)
+    forcing = fc.Forcing(
+        flow_idx=arr(f.flow_idx, f.n_flow, np.int32), flow_type=arr(f.flow_type, f.n_flow, np.int32),
+        flow_value=arr(f.flow_value, f.n_flow, np.float64), flow_off=fo,
+        flow_times=arr(f.flow_times, int(fo[-1]) if len(fo) else 0, np.float64),
+        flow_vals=arr(f.flow_vals, int(fo[-1]) if len(fo) else 0, np.float64),
+        other_idx=arr(f.other_idx, f.n_other, np.int32),
+        other_type=arr(f.other_type, f.n_other, np.int32),
+        other_value=arr(f.other_value, f.n_other, np.float64), other_off=oo,
+        other_times=arr(f.other_times, int(oo[-1]) if len(oo) else 0, np.float64),
+        other_vals=arr(f.other_vals, int(oo[-1]) if len(oo) else 0, np.float64),
+        rain_times=arr(f.rain_times, f.n_rain, np.float64),
+        rain_rates=arr(f.rain_rates, f.n_rain, np.float64))
+    case = sc.Case(nx, ny, d.dx, dem, xll=float(geo[0]), yll=float(geo[1]), nodata=d.nodata,
+                   sim_time=float(par[0]), save_int=float(par[1]), mass_int=float(par[2]),
+                   init_tstep=d.init_tstep, cfl=d.cfl, fpn=d.fpn, depth_thresh=d.depth_thresh,
+                   west_free=bool(d.west_free), east_free=bool(d.east_free),
+                   north_free=bool(d.north_free), south_free=bool(d.south_free),
+                   name=path)
+    if forcing.n_rain:
+        case.rain_times, case.rain_rates = forcing.rain_times, forcing.rain_rates
+    return case, forcing
 
 
 def par_outputs(path: str) -> dict:
@@ -272,8 +282,7 @@ def par_outputs(path: str) -> dict:
     (af_scenario_output): out_dir, save_int, voutput, async_style,
     output_format, stage_int and the stage points [(name, cell index or -1)]."""
     lib = _lib.lib()
-    h = C.c_void_p()
-    _lib.check(lib.af_scenario_load(path.encode(), C.byref(h)), "af_scenario_load " + path)
+    h = _open_par(path)
     try:
         o = _lib.OutputDesc()
         _lib.check(lib.af_scenario_output(h, C.byref(o)), "af_scenario_output")
@@ -291,11 +300,10 @@ def run_par(path: str, precision: str = "f64", device: int = 0) -> int:
     """Runs a ``.par`` case as the reference's CLI does (src/main.cpp): reads
     its inputs, steps it to sim_time and writes the files it asks for
     (af_sim_run_output with af_scenario_output).  Returns the steps taken."""
-    case, forcing = load_par(path)
     lib = _lib.lib()
-    h = C.c_void_p()
-    _lib.check(lib.af_scenario_load(path.encode(), C.byref(h)), "af_scenario_load " + path)
+    h = _open_par(path)
     try:
+        case, forcing = _case_of(h, path)
         o = _lib.OutputDesc()
         _lib.check(lib.af_scenario_output(h, C.byref(o)), "af_scenario_output")
         with Simulation(case, precision, device=device, forcing=forcing) as s:
