@@ -80,6 +80,7 @@ _SIGS = {
     "af_add_point_sources_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "af_volume_area": (_i, [_vp, _i64, _d, _vp, _vp, _vp]),
     "af_fill": (_i, [_vp, _i64, _d, _vp]),
+    "af_pow_eval": (_i, [_vp, _vp, _i64, _d, _vp]),
     "af_sim_create": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
     "af_sim_destroy": (_i, [_vp]),
     "af_sim_launch": (_i, [_vp, _d, _i64]),

@@ -39,7 +39,7 @@ UNITS = [
     ("af_xfer.cu", EXACT),
 ]
 HOST_UNITS = ["af_io.cpp", "af_arena.cpp", "af_output.cpp"]
-HEADERS = ["af_common.cuh", "af_step.cuh", "af_simcore.cuh", "af_arena.h", "af_output.h",
+HEADERS = ["af_common.cuh", "af_pow.cuh", "af_pow_tables.h", "af_step.cuh", "af_simcore.cuh", "af_arena.h", "af_output.h",
            "af_xfer.h"]
 
 

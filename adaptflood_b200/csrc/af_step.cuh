@@ -35,6 +35,7 @@
 #include <cstdint>
 
 #include "af_common.cuh"
+#include "af_pow.cuh"
 
 namespace af {
 
@@ -235,7 +236,8 @@ __device__ inline T bc_depth(int b, SeriesTable tb, double t) {
 // `if (Q*dh < 0)` recomputation (src/kernels.cpp:86-89) yields the same Q
 // (both numerators are equal whenever Q != 0), so it is not repeated.
 
-// FP64: the reference's expressions exactly (src/kernels.cpp:60-84).
+// FP64: the reference's expressions exactly (src/kernels.cpp:60-84), with the
+// C library's pow algorithm (af_pow.cuh).
 __device__ inline void row_faces(const double (&h)[2], const double (&z)[2], const double (&hN)[2],
                                  const double (&zN)[2], const double (&qxo)[2],
                                  const double (&qxoN)[2], const double (&qyo)[2],
@@ -278,7 +280,7 @@ __device__ inline void row_faces(const double (&h)[2], const double (&z)[2], con
       const double qvect = sqrt(Q0[f] * Q0[f] + qy_avg * qy_avg);
       const double numerator = (Q0[f] + 0.0) - (ph.gdt * hflow * Sf);
       const double denominator =
-          1.0 + ph.gdt * hflow * ph.fn * ph.fn * fabs(qvect) / pow(hflow, 10.0 / 3.0);
+          1.0 + ph.gdt * hflow * ph.fn * ph.fn * fabs(qvect) / pw::pow_ref(hflow, 10.0 / 3.0);
       const double q = numerator / denominator * ph.dx;
       Q[f] = wet[f] ? q : 0.0;
     }

@@ -144,6 +144,14 @@ int af_volume_area(const double* H, int64_t n, double dA, double* vol, double* a
 /* Replaces the inline Init* fills of src/main.cpp:156-160. */
 int af_fill(double* x, int64_t n, double value, void* stream);
 
+/* No counterpart in the reference's interface: evaluates, over a device
+ * array, the pow that the FP64 kernels use for the friction term's
+ * pow(hflow, 10.0/3.0) (src/kernels.cpp:83,133): out[k] = x[k]^y.  It is the
+ * C library's (glibc >= 2.28) table-driven algorithm restated, and returns
+ * glibc's value on all but about 1e-7 of positive normal arguments; a caller
+ * can compare it with its own C library here.  Synchronous on `stream`. */
+int af_pow_eval(const double* x, double* out, int64_t n, double y, void* stream);
+
 /* ================================================== 2. simulation layer == */
 
 enum { AF_PREC_F64 = 0, AF_PREC_F32 = 1 };

@@ -23,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libaforacle.so")
 REF_SO = os.path.join(HERE, "_ref", "libafref.so")
 REF_CLI = os.path.join(HERE, "_ref", "lisflood_ref")
+POW_SO = os.path.join(HERE, "_build", "libpowcheck.so")
 _lock = threading.Lock()
 _libs = {}
 
@@ -74,6 +75,27 @@ def _oracle_lib():
         lib.afo_get.argtypes = [C.c_void_p] + [C.c_void_p] * 5
         lib.afo_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]
         _libs["oracle"] = lib
+        return lib
+
+
+def pow_check_lib():
+    """The C library's pow and the host build of the restated pow
+    (``pow_check.cpp``), over arrays."""
+    with _lock:
+        if "pow" in _libs:
+            return _libs["pow"]
+        srcs = [os.path.join(HERE, "pow_check.cpp"),
+                os.path.join(HERE, "..", "adaptflood_b200", "csrc", "af_pow.cuh"),
+                os.path.join(HERE, "..", "adaptflood_b200", "csrc", "af_pow_tables.h")]
+        if _stale(POW_SO, srcs):
+            _make("_build/libpowcheck.so")
+        lib = C.CDLL(POW_SO)
+        for fn in (lib.powc_libc, lib.powc_restated):
+            fn.restype = None
+            fn.argtypes = [C.c_void_p, C.c_void_p, C.c_long, C.c_double]
+        lib.powc_mismatch.restype = C.c_long
+        lib.powc_mismatch.argtypes = [C.c_void_p, C.c_long, C.c_double]
+        _libs["pow"] = lib
         return lib
 
 

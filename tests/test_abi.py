@@ -45,6 +45,8 @@ def test_validation_without_device():
     assert lib.af_update_qs(None, None, None, None, 65535, 65535, 1.0, None) == _lib.AF_ERANGE
     assert lib.af_fill(None, -5, 0.0, None) == _lib.AF_EINVAL
     assert lib.af_fill(None, 0, 0.0, None) == _lib.AF_OK
+    assert lib.af_pow_eval(None, None, -1, 2.0, None) == _lib.AF_EINVAL
+    assert lib.af_pow_eval(None, None, 0, 2.0, None) == _lib.AF_OK
     assert lib.af_add_point_sources(None, None, None, 0, 10, None) == _lib.AF_OK
     assert lib.af_apply_point_bcs(None, None, None, None, -1, 0, 1.0, 1.0, 1.0, 10,
                                   None) == _lib.AF_EINVAL
