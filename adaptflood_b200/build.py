@@ -95,5 +95,16 @@ def build(verbose: bool = False, ptxas_info: bool = False, obj_dir: str = None, 
     return text
 
 
+# A test build whose ring waits give up at once (AF_RING_WAIT_LIMIT=0): the
+# failure tests run the kernels' time-out path with it (the warp drains its
+# copies, flags the control block, and the loop stops with AF_ESTATE).
+WAITTEST_LIB = os.path.join(HERE, "libadaptflood_waittest.so")
+
+
+def build_wait_test(verbose: bool = False) -> str:
+    return build(verbose=verbose, obj_dir=os.path.join(HERE, "_build_waittest"), lib=WAITTEST_LIB,
+                 defines=("AF_RING_WAIT_LIMIT=0",))
+
+
 if __name__ == "__main__":
     print(build(verbose=False, ptxas_info="--ptxas" in sys.argv) or "up to date")

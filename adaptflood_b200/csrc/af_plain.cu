@@ -759,24 +759,17 @@ constexpr int kNoAllocMaxSources = AF_NOALLOC_MAX_SOURCES;
 // 32 words (256 bytes) of header -- the error flag in word 0 -- then the keys.
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[32 + kNoAllocMaxSources];
 
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[64] = {};
-
-// The device address of g_noalloc_scratch on the current device.  In host code
-// the symbol names a host-side shadow, not device memory, so the address has
-// to be looked up once per device (with that device current).
+// The device address of g_noalloc_scratch in the current device's context.
+// In host code the symbol names a host-side shadow, not device memory, so the
+// address is looked up with the device current -- on every call, not cached:
+// a cached address would outlive a cudaDeviceReset (which unloads the module
+// and places the array anew when it is next loaded).  The lookup neither
+// allocates nor synchronises once the module is loaded on the device.
 int noalloc_scratch(unsigned long long** out) {
-  int dev = 0;
-  AF_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return AF_EINVAL;
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_fail(e);
-    g_noalloc_addr[dev] = p;
-  }
-  *out = static_cast<unsigned long long*>(g_noalloc_addr[dev]);
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_fail(e);
+  *out = static_cast<unsigned long long*>(p);
   return AF_OK;
 }
 

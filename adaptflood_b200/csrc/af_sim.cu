@@ -175,7 +175,8 @@ __global__ void k_begin(SimCtl* ctl, double t_stop, long long max_steps,
   long long s = ctl->step;
   ctl->step_stop = (max_steps > (long long)0x3FFFFFFFFFFFFFFFLL - s) ? 0x3FFFFFFFFFFFFFFFLL
                                                                       : s + max_steps;
-  int done = !(ctl->t < t_stop) || max_steps <= 0;
+  // A simulation whose state went bad stays stopped (no further steps).
+  int done = !(ctl->t < t_stop) || max_steps <= 0 || ctl->status != 0;
   ctl->done = done;
   ctl->arrive = 0u;
   if (use_cond) cudaGraphSetConditional(cond, done ? 0u : 1u);
@@ -250,6 +251,7 @@ struct Sim {
   bool use_cond = false;
   int n_rain = 0;
   std::vector<double> rain_t, rain_r;
+  uint64_t case_hash = 0;  // case parameters and forcing (checkpoint identity)
 
   ~Sim() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -465,6 +467,76 @@ static int build_graph(Sim& s) {
   return AF_OK;
 }
 
+// Identity of a case for checkpoints: a 64-bit mix (splitmix64 finaliser)
+// of every parameter and forcing value, position by position.
+static inline uint64_t mix64(uint64_t x) {
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ULL;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebULL;
+  return x ^ (x >> 31);
+}
+struct Hasher {
+  uint64_t h = 0x6166636b70743032ULL, n = 0;
+  void word(uint64_t w) { h = mix64(h ^ mix64(w + 0x9e3779b97f4a7c15ULL * ++n)); }
+  void d(double v) {
+    uint64_t w;
+    memcpy(&w, &v, 8);
+    word(w);
+  }
+  void i(long long v) { word((uint64_t)v); }
+  template <typename T>
+  void arr(const T* a, long long k) {
+    i(k);
+    for (long long q = 0; q < (a ? k : 0); q++) {
+      if (sizeof(T) == 8) d((double)a[q]);
+      else i((long long)a[q]);
+    }
+  }
+};
+static uint64_t case_hash(const af_case_desc* c, const af_forcing_desc* f) {
+  Hasher h;
+  h.i(c->nx); h.i(c->ny);
+  h.d(c->dx); h.d(c->nodata); h.d(c->fpn); h.d(c->depth_thresh); h.d(c->cfl);
+  h.d(c->init_tstep); h.d(c->g); h.d(c->max_hflow); h.d(c->theta); h.d(c->mass_int);
+  h.i(c->west_free); h.i(c->east_free); h.i(c->north_free); h.i(c->south_free);
+  const int nf = f->n_flow, no = f->n_other;
+  const long long fser = (nf > 0 && f->flow_off) ? f->flow_off[nf] : 0;
+  const long long oser = (no > 0 && f->other_off) ? f->other_off[no] : 0;
+  h.arr(f->flow_idx, nf); h.arr(f->flow_type, nf); h.arr(f->flow_value, nf);
+  h.arr(f->flow_off, nf > 0 ? nf + 1 : 0); h.arr(f->flow_times, fser); h.arr(f->flow_vals, fser);
+  h.arr(f->other_idx, no); h.arr(f->other_type, no); h.arr(f->other_value, no);
+  h.arr(f->other_off, no > 0 ? no + 1 : 0); h.arr(f->other_times, oser);
+  h.arr(f->other_vals, oser);
+  h.arr(f->rain_times, f->n_rain); h.arr(f->rain_rates, f->n_rain);
+  return h.h;
+}
+
+// Order-free hash of the stored DEM: the wrapping sum over valid cells of a
+// mix of (value bits, cell index), so the result does not depend on the
+// launch shape.
+template <typename T>
+__global__ void k_dem_hash(const T* __restrict__ Z, int nx, int ny, int P,
+                           unsigned long long* out) {
+  const long long n = (long long)nx * ny;
+  unsigned long long acc = 0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(k / nx), i = (int)(k - (long long)j * nx);
+    unsigned long long w;
+    if (sizeof(T) == 8) w = (unsigned long long)__double_as_longlong((double)Z[(long long)j * P + i]);
+    else w = (unsigned long long)__float_as_uint((float)Z[(long long)j * P + i]);
+    unsigned long long x = w ^ (0x9e3779b97f4a7c15ULL * (unsigned long long)(k + 1));
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ULL;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebULL;
+    acc += x ^ (x >> 31);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
 static int create(const af_case_desc* c, const af_forcing_desc* f, const double* dem,
                   const double* h0, int precision, int device, Sim** out) {
   if (!c || !f || !dem || !out) return AF_EINVAL;
@@ -477,6 +549,7 @@ static int create(const af_case_desc* c, const af_forcing_desc* f, const double*
   s->esize = precision == AF_PREC_F64 ? 8 : 4;
   s->N = 16 / s->esize;
   s->c = *c;
+  s->case_hash = case_hash(c, f);
   AF_CUDA(cudaSetDevice(device));
   AF_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
   AF_CUDA(cudaMallocHost(&s->pinned_ctl, sizeof(SimCtl)));
@@ -1038,12 +1111,35 @@ static int run_output(Sim& s, double sim_time, const af_output_desc& o, int64_t*
   return writer.errors() ? AF_EIO : AF_OK;
 }
 
-// Checkpoint file: "AFCKPT01", int32 precision, nx, ny, mass count, the
-// control block (SimCtl, native layout), the mass series (3 doubles per
-// entry), then H (ny x nx), Qx (ny x (nx+1)) and Qy ((ny+1) x nx) in the state
-// precision, dense.  Native byte order: a checkpoint is read back on the same
-// kind of host it was written on.
-static const char kCkptMagic[8] = {'A', 'F', 'C', 'K', 'P', 'T', '0', '1'};
+// Checkpoint file: "AFCKPT02", int32 precision, nx, ny, mass count, uint32
+// sizeof(SimCtl), uint32 0, uint64 hash of the case parameters and forcing,
+// uint64 hash of the stored DEM, the control block (SimCtl, native layout),
+// the mass series (3 doubles per entry), then H (ny x nx), Qx (ny x (nx+1))
+// and Qy ((ny+1) x nx) in the state precision, dense.  Native byte order: a
+// checkpoint is read back on the same kind of host it was written on.  A
+// restore into another case (grid, parameters, forcing or DEM), precision or
+// build whose control block differs is refused with AF_EINVAL.
+static const char kCkptMagic[8] = {'A', 'F', 'C', 'K', 'P', 'T', '0', '2'};
+
+// (The accumulator is the first word of the step's partials buffer, which
+// holds nothing between launches; stream order puts this after any step.)
+static int dem_hash(Sim& s, uint64_t* out) {
+  DevBuf& acc = s.partials;
+  AF_CUDA(cudaMemsetAsync(acc.p, 0, 8, s.st));
+  const long long n = (long long)s.c.nx * s.c.ny;
+  const unsigned grid = grid_for(n, 256, 4);
+  unsigned long long* a = static_cast<unsigned long long*>(acc.p);
+  if (s.prec == AF_PREC_F64)
+    k_dem_hash<double><<<grid, 256, 0, s.st>>>(s.buf<double>(s.DEM), s.c.nx, s.c.ny, s.P, a);
+  else
+    k_dem_hash<float><<<grid, 256, 0, s.st>>>(s.buf<float>(s.DEM), s.c.nx, s.c.ny, s.P, a);
+  AF_CUDA(cudaGetLastError());
+  unsigned long long h = 0;
+  AF_CUDA(cudaMemcpyAsync(&h, acc.p, 8, cudaMemcpyDeviceToHost, s.st));
+  AF_CUDA(cudaStreamSynchronize(s.st));
+  *out = h;
+  return AF_OK;
+}
 
 static int field_io(Sim& s, DevBuf& b, std::vector<char>& host, int rows, int width, bool put) {
   char* dev = static_cast<char*>(b.p) + (size_t)kGuard * s.esize;
@@ -1072,7 +1168,11 @@ static int checkpoint(Sim& s, const char* path) {
   if (!f) return AF_EIO;
   std::unique_ptr<FILE, int (*)(FILE*)> guard(f, fclose);
   const int32_t hdr[4] = {s.prec, nx, ny, nm};
+  const uint32_t sizes[2] = {(uint32_t)sizeof(SimCtl), 0u};
+  uint64_t ids[2] = {s.case_hash, 0};
+  AF_TRY(dem_hash(s, &ids[1]));
   bool ok = fwrite(kCkptMagic, 1, 8, f) == 8 && fwrite(hdr, sizeof hdr, 1, f) == 1 &&
+            fwrite(sizes, sizeof sizes, 1, f) == 1 && fwrite(ids, sizeof ids, 1, f) == 1 &&
             fwrite(&ctl, sizeof ctl, 1, f) == 1 &&
             (nm == 0 || fwrite(mass.data(), 8, mass.size(), f) == mass.size());
   const int shape[3][2] = {{ny, nx}, {ny, nx + 1}, {ny + 1, nx}};
@@ -1093,14 +1193,22 @@ static int restore(Sim& s, const char* path) {
   std::unique_ptr<FILE, int (*)(FILE*)> guard(f, fclose);
   char magic[8];
   int32_t hdr[4];
+  uint32_t sizes[2];
+  uint64_t ids[2];
   SimCtl ctl;
   if (fread(magic, 1, 8, f) != 8 || memcmp(magic, kCkptMagic, 8) != 0 ||
-      fread(hdr, sizeof hdr, 1, f) != 1 || fread(&ctl, sizeof ctl, 1, f) != 1)
+      fread(hdr, sizeof hdr, 1, f) != 1 || fread(sizes, sizeof sizes, 1, f) != 1 ||
+      fread(ids, sizeof ids, 1, f) != 1)
     return AF_EIO;
   const int nx = s.c.nx, ny = s.c.ny;
-  if (hdr[0] != s.prec || hdr[1] != nx || hdr[2] != ny || hdr[3] < 0 || hdr[3] > kMassCap ||
-      ctl.parity < 0 || ctl.parity > 1)
-    return AF_EINVAL;  // another case or precision
+  if (sizes[0] != (uint32_t)sizeof(SimCtl) || hdr[0] != s.prec || hdr[1] != nx ||
+      hdr[2] != ny || hdr[3] < 0 || hdr[3] > kMassCap || ids[0] != s.case_hash)
+    return AF_EINVAL;  // another case, precision or control-block layout
+  uint64_t dem_id = 0;
+  AF_TRY(dem_hash(s, &dem_id));
+  if (ids[1] != dem_id) return AF_EINVAL;  // another DEM
+  if (fread(&ctl, sizeof ctl, 1, f) != 1) return AF_EIO;
+  if (ctl.parity < 0 || ctl.parity > 1) return AF_EINVAL;
   std::vector<double> mass((size_t)hdr[3] * 3);
   if (!mass.empty() && fread(mass.data(), 8, mass.size(), f) != mass.size()) return AF_EIO;
   const int par = ctl.parity;

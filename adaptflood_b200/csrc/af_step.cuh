@@ -383,6 +383,14 @@ constexpr int kStages = AF_STAGES;  // ring depth (rows in flight per warp, incl
 constexpr int kRowUnroll = AF_ROW_UNROLL;
 constexpr int kRowBytes = 512;
 constexpr long long kWaitLimit = 1LL << 22;
+// Polls a warp spends waiting for a row of its ring before it gives up (the
+// drain after a give-up keeps kWaitLimit).  A test build sets it to 0, so
+// every such wait runs out at once and the time-out path is exercised without
+// a slow or stuck copy.
+#ifndef AF_RING_WAIT_LIMIT
+#define AF_RING_WAIT_LIMIT (1LL << 22)
+#endif
+constexpr long long kRingWaitLimit = AF_RING_WAIT_LIMIT;
 
 __device__ inline uint32_t smem_u32(const void* ptr) {
   return (uint32_t)__cvta_generic_to_shared(ptr);
@@ -414,9 +422,10 @@ __device__ inline bool mbar_try_wait(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// True once every lane has seen the phase complete; false after kWaitLimit polls.
-__device__ inline bool mbar_wait_warp(uint64_t* b, uint32_t parity) {
-  for (int i = 0; i < (int)kWaitLimit; i++) {
+// True once every lane has seen the phase complete; false after `limit` polls.
+__device__ inline bool mbar_wait_warp(uint64_t* b, uint32_t parity,
+                                      long long limit = kWaitLimit) {
+  for (int i = 0; i < (int)limit; i++) {
     const bool ok = mbar_try_wait(b, parity);
     if (__all_sync(0xffffffffu, ok)) return true;
   }
@@ -619,7 +628,8 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
   int kc = 0;  // next stage of this strip to consume
   auto acquire = [&]() -> const unsigned char* {
     const int q = kglob + kc;
-    if (!mbar_wait_warp(&bar[q % kStages], (uint32_t)((q / kStages) & 1))) return nullptr;
+    if (!mbar_wait_warp(&bar[q % kStages], (uint32_t)((q / kStages) & 1), kRingWaitLimit))
+      return nullptr;
     return &ring[q % kStages][0][0] + lane * 16;
   };
   auto release = [&]() {

@@ -181,7 +181,7 @@ def cpu_reference(case, forcing, h0, seconds: float, max_steps: int):
             "kind": "reference", "steps": n, "seconds": el,
             "sample": f"{n} steps of the same {case.nx}x{case.ny} workload from the same start "
                       f"state (after 1 warm-up step), reference src/kernels.cpp + main.cpp loop "
-                      f"compiled -O2 -fopenmp against the Kokkos-API shim"}
+                      f"compiled -O3 -fopenmp against the Kokkos-API shim"}
 
 
 def run_reference(args, rank: int, world: int):

@@ -125,9 +125,11 @@ int af_add_point_sources(double* H, const int* ps_idx, const double* ps_flow, in
  *     AF_ERANGE before anything runs, and H is left unchanged.  Indices off
  *     the grid are skipped and reported with AF_ERANGE, as in
  *     af_add_point_sources.
- *   - The first call on each device looks up the array's device address on
- *     that device (with it current); make that first call before any stream
- *     capture.
+ *   - Each call looks up the array's device address on the current device
+ *     (the first call on a device loads the library's device code there),
+ *     then waits for `stream` before it returns (it reads an error flag back
+ *     to the host): the call is synchronous, and it must not be made while
+ *     `stream` is being captured into a graph.
  *   - Every call shares the one array: calls whose work overlaps on the GPU
  *     (concurrent streams or host threads) race and must be serialised by
  *     the caller.  Each call clears the state it relies on. */

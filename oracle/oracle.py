@@ -31,8 +31,17 @@ _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
 
-def _make(target: str) -> None:
-    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+def _make(target: str, ref_dir: str = None) -> None:
+    cmd = ["make", "-s", "-C", HERE, target]
+    if ref_dir:
+        cmd.append("REF=" + ref_dir)
+    subprocess.run(cmd, check=True)
+
+
+def reference_dir():
+    """The reference checkout named by AF_REFERENCE_DIR, if it exists here."""
+    d = os.environ.get("AF_REFERENCE_DIR")
+    return d if d and os.path.isdir(d) else None
 
 
 def _stale(so: str, sources) -> bool:
@@ -42,12 +51,13 @@ def _stale(so: str, sources) -> bool:
     return any(os.path.exists(s) and os.path.getmtime(s) > t for s in sources)
 
 
-def build(ref: bool = True) -> None:
-    """Compile the C restatement and, where the reference is mounted, the
-    reference library and CLI."""
+def build(ref: bool = True, ref_dir: str = None) -> None:
+    """Compile the C restatement and, given the reference checkout (`ref_dir`
+    or AF_REFERENCE_DIR), the reference library and CLI."""
     _make("oracle")
-    if ref and os.path.isdir(os.environ.get("AF_REFERENCE_DIR", "/root/reference")):
-        _make("ref")
+    d = ref_dir or reference_dir()
+    if ref and d and os.path.isdir(d):
+        _make("ref", d)
 
 
 def _oracle_lib():

@@ -70,3 +70,64 @@ def test_two_gloo_ranks_run_their_shares_and_gather_all(tmp_path):
         for k, v in res.items():
             assert v["rank"] == next(q for q in range(world) if k in shares[q])
             assert v["steps"] == math.ceil(cases[k].sim_time / 7.0) and v["state"] == 1
+
+
+class _FailingBatch:
+    """A batch whose admission fails (as Batch.add does when the device
+    refuses), on one rank only."""
+
+    def try_add(self, case, forcing=None, t_stop=None):
+        raise RuntimeError("admission failed on purpose")
+
+    def close(self):
+        pass
+
+
+def _rank_fail_main(rank, world, port, out_dir):
+    import sys
+    import torch.distributed as dist
+    from datetime import timedelta
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from _fakes import FakeBatch
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world, timeout=timedelta(seconds=60))
+    try:
+        factory = (lambda: _FailingBatch()) if rank == 1 else (
+            lambda: FakeBatch(arena_bytes=1 << 30, dt=7.0))
+        try:
+            dispatch.run_ensemble(_cases(), rank, world, dist, batch_factory=factory)
+            msg = "returned"
+        except RuntimeError as e:
+            msg = str(e)
+        with open(os.path.join(out_dir, f"r{rank}.txt"), "w") as f:
+            f.write(msg)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_a_failing_rank_makes_every_rank_raise(tmp_path):
+    import time
+    world = 2
+    t0 = time.time()
+    mp.spawn(_rank_fail_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    assert time.time() - t0 < 50  # well inside the process group's timeout
+    for r in range(world):
+        msg = open(tmp_path / f"r{r}.txt").read()
+        assert "rank 1: RuntimeError: admission failed on purpose" in msg
+
+
+def test_a_share_larger_than_the_arena_runs_in_waves():
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from _fakes import FakeBatch
+    cases = _cases()
+    biggest = max(c.cells for c in cases) * 28
+    fb = FakeBatch(arena_bytes=3 * biggest, dt=7.0)
+    res = dispatch.run_ensemble(cases, 0, 1, None, batch_factory=lambda: fb)
+    assert sorted(res) == list(range(len(cases)))
+    for k, v in res.items():
+        assert v["steps"] == math.ceil(cases[k].sim_time / 7.0) and v["state"] == 1
+    assert fb.peak_used <= 3 * biggest and not fb.slots  # every slot freed
+    with pytest.raises(MemoryError):
+        dispatch.run_ensemble(cases, 0, 1, None,
+                              batch_factory=lambda: FakeBatch(arena_bytes=biggest // 2, dt=7.0))

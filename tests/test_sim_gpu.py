@@ -12,6 +12,7 @@ import pytest
 from _util import golden_names, load_golden
 from adaptflood_b200 import forcing as fc
 from adaptflood_b200 import scenarios as sc
+from adaptflood_b200 import _lib
 from adaptflood_b200._lib import AFError
 from adaptflood_b200.sim import Simulation
 from oracle import oracle as orc
@@ -305,6 +306,19 @@ def test_checkpoint_restart_is_bit_identical(cuda, tmp_path, prec):
             d.restore(ck)
         with pytest.raises(AFError):
             d.restore(str(tmp_path / "missing.ckpt"))
+    # same grid size, another case: a different DEM, Manning n, or forcing
+    import copy
+    dem2 = copy.copy(case)
+    dem2.dem = case.dem.copy()
+    dem2.dem[10, 20] += 0.25
+    fpn2 = copy.copy(case)
+    fpn2.fpn = case.fpn * 1.5
+    for other_case, other_f in ((dem2, f), (fpn2, f), (case, fc.pack(sc.small_case(
+            131, 77, seed=63, rain=True, n_hvar=1, n_qvar=2, sim_time=400.0)))):
+        with Simulation(other_case, prec, forcing=other_f) as e:
+            with pytest.raises(AFError) as err:
+                e.restore(ck)
+            assert err.value.code == _lib.AF_EINVAL
 
 
 def test_step_limits_are_exact(cuda):

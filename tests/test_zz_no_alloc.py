@@ -4,9 +4,10 @@ their own pool, or cannot afford the device-wide synchronisation of cudaFree).
 
 Checked through the C ABI against af_add_point_sources on the same inputs,
 bit for bit, on two calls in a row (the calls share one fixed device array,
-so the second call must not see anything the first left behind).  This file
-is collected last on purpose; it passes alone in a fresh process and after
-the other tests.
+so the second call must not see anything the first left behind), and against
+the reference's sequential scatter (src/main.cpp:256-260 in file order)
+computed on the CPU.  This file is collected last on purpose; it passes
+alone in a fresh process and after the other tests.
 """
 import ctypes as C
 
@@ -37,6 +38,19 @@ def _case(seed, n, ncell, bad=False):
             torch.from_numpy(flow).cuda())
 
 
+def _sequential(H, idx, flow, ncell):
+    """The reference's scatter, one source after another in file order,
+    skipping indices off the grid."""
+    out = H.copy()
+    for k in range(idx.size):
+        i = int(idx[k])
+        if 0 <= i < ncell:
+            out[i] += flow[k]
+            if out[i] < 0.0:
+                out[i] = 0.0
+    return out
+
+
 def test_noalloc_matches_allocating_entry_point_on_consecutive_calls(cuda):
     lib = _lib.lib()
     max_n = 4096
@@ -49,6 +63,8 @@ def test_noalloc_matches_allocating_entry_point_on_consecutive_calls(cuda):
         rc_got = _call(lib.af_add_point_sources_noalloc, got, idx, flow, n, ncell)
         assert rc_got == rc_want == (_lib.AF_ERANGE if bad else _lib.AF_OK)
         assert bool((got == want).all()), f"seed {seed}"
+        seq = _sequential(H0.cpu().numpy(), idx.cpu().numpy(), flow.cpu().numpy(), ncell)
+        np.testing.assert_array_equal(got.cpu().numpy(), seq)
 
 
 def test_noalloc_rejects_more_than_the_maximum(cuda):
