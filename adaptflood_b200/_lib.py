@@ -118,6 +118,8 @@ _SIGS = {
     "af_batch_get_state": (_i, [_vp, _i, _vp, _vp, _vp]),
     "af_batch_mass_series": (_i, [_vp, _i, _vp, _vp, _vp, _i, _vp]),
     "af_batch_info": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "af_batch_set_trace": (_i, [_vp, _i64]),
+    "af_batch_get_trace": (_i, [_vp, _vp, _i64, _vp]),
     "af_batch_stream": (_vp, [_vp]),
     "af_arena_create": (_i, [_u64, _vp]),
     "af_arena_destroy": (_i, [_vp]),

@@ -187,6 +187,20 @@ class Batch:
                                                  C.byref(n)), "af_batch_mass_series")
         return t[:k], v[:k], a[:k]
 
+    def set_trace(self, cap: int) -> None:
+        """Records up to `cap` batch steps from now (0: off); see trace()."""
+        _lib.check(self.lib.af_batch_set_trace(self.h, int(cap)), "af_batch_set_trace")
+
+    def trace(self) -> np.ndarray:
+        """The recorded steps since set_trace, one row each: start and end on
+        the device clock (ns), cells and strips stepped."""
+        n = C.c_int64()
+        _lib.check(self.lib.af_batch_get_trace(self.h, None, 0, C.byref(n)), "af_batch_get_trace")
+        out = np.zeros((max(n.value, 1), 4), dtype=np.int64)
+        _lib.check(self.lib.af_batch_get_trace(self.h, _p(out), n.value, C.byref(n)),
+                   "af_batch_get_trace")
+        return out[:n.value]
+
     def info(self) -> dict:
         m = C.c_int()
         st = C.c_int64()

@@ -26,6 +26,7 @@
 //   * af_batch_get_state may run while a launch is in flight for a scenario
 //     that had finished at the last sync (it is no longer stepped).
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -157,6 +158,7 @@ struct Batch {
   BatchCtl* h_bctl = nullptr;
   int* h_attn = nullptr;      // mapped pinned attention flag
   int* d_attn = nullptr;
+  unsigned long long* d_trace = nullptr;  // per-step trace records (af_batch_set_trace)
   BatchParams bp{};
   dim3 grid, block;
   cudaGraph_t graph = nullptr;
@@ -183,6 +185,7 @@ struct Batch {
     if (d_ctl) cudaFree(d_ctl);
     if (d_tab) cudaFree(d_tab);
     if (d_bctl) cudaFree(d_bctl);
+    if (d_trace) cudaFree(d_trace);
     if (h_ctl) cudaFreeHost(h_ctl);
     if (h_tab) cudaFreeHost(h_tab);
     if (h_bctl) cudaFreeHost(h_bctl);
@@ -852,6 +855,46 @@ int af_batch_mass_series(af_batch* h, int slot, double* t, double* vol, double* 
     if (area) area[k] = buf[3 * k + 2];
   }
   *n = b.h_ctl[slot].mass_count;
+  return AF_OK;
+}
+
+int af_batch_set_trace(af_batch* h, int64_t cap) {
+  if (!h || cap < 0) return AF_EINVAL;
+  Batch& b = *h->b;
+  if (b.in_flight) return AF_ESTATE;
+  AF_CUDA(cudaSetDevice(b.device));
+  AF_CUDA(cudaStreamSynchronize(b.st));
+  if (b.d_trace) {
+    AF_CUDA(cudaFree(b.d_trace));
+    b.d_trace = nullptr;
+  }
+  if (cap > 0) AF_TRY(af::alloc_dev((void**)&b.d_trace, (size_t)cap * 32));
+  af::BatchCtl& c = *b.h_bctl;
+  c.trace = b.d_trace;
+  c.trace_base = c.step;
+  c.trace_cap = cap;
+  const size_t off = offsetof(af::BatchCtl, trace);
+  AF_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(b.d_bctl) + off,
+                          reinterpret_cast<char*>(&c) + off, sizeof(af::BatchCtl) - off,
+                          cudaMemcpyHostToDevice, b.st));
+  AF_CUDA(cudaStreamSynchronize(b.st));
+  return AF_OK;
+}
+
+int af_batch_get_trace(af_batch* h, int64_t* rec, int64_t cap, int64_t* n) {
+  if (!h || !n || cap < 0 || (cap > 0 && !rec)) return AF_EINVAL;
+  Batch& b = *h->b;
+  if (b.in_flight) return AF_ESTATE;
+  const af::BatchCtl& c = *b.h_bctl;
+  long long have = b.d_trace ? std::min(c.step - c.trace_base, c.trace_cap) : 0;
+  if (have < 0) have = 0;
+  *n = have;
+  const long long k = std::min<long long>(have, cap);
+  if (k > 0) {
+    AF_CUDA(cudaSetDevice(b.device));
+    AF_CUDA(cudaMemcpyAsync(rec, b.d_trace, (size_t)k * 32, cudaMemcpyDeviceToHost, b.st));
+    AF_CUDA(cudaStreamSynchronize(b.st));
+  }
   return AF_OK;
 }
 

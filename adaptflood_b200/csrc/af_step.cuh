@@ -1066,6 +1066,7 @@ struct BatchTab {
   int member[kMaxSlots];
   int nact;                   // scenarios stepped by the coming step
   int units;                  // their strips
+  long long cells;            // their cells
   int act[kMaxSlots];         // their slots
   int u0[kMaxSlots + 1];      // first unit of each; u0[nact] = units
 };
@@ -1077,7 +1078,19 @@ struct BatchCtl {
   int stop_on_done;
   int done;             // or when nothing is active or the host asks for attention
   int status;           // nonzero: a wait timed out; the batch's state is invalid
+  // Optional per-step trace (af_batch_set_trace): record k describes batch
+  // step trace_base + k as {start, end} on the device clock (ns) and the
+  // cells and strips it stepped.  Written by the host between launches.
+  unsigned long long* trace;
+  long long trace_base, trace_cap;
+  unsigned long long last_stamp;  // end of the previous step, or the launch's start
 };
+
+__device__ inline unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 struct BatchParams {
   BatchScen* scen;                 // per slot
@@ -1095,6 +1108,7 @@ __device__ inline void batch_compact(const BatchParams& bp) {
   const int lane = threadIdx.x & 31;
   const int nm = tab->nmember;
   int nact = 0, units = 0;
+  long long cells = 0;
   for (int base = 0; base < nm; base += 32) {
     const int i = base + lane;
     int slot = -1, nu = 0;
@@ -1106,6 +1120,7 @@ __device__ inline void batch_compact(const BatchParams& bp) {
       act = __ldcg(&c->status) == 0 && __ldcg(&c->t) < __ldcg(&c->t_stop) &&
             __ldcg(&c->step) < __ldcg(&c->step_stop);
       nu = sp->nsx * sp->nsy;
+      if (act) cells += (long long)sp->nx * sp->ny;
     }
     const unsigned m = __ballot_sync(0xffffffffu, act);
     int x = act ? nu : 0;  // inclusive scan of the active lanes' strip counts
@@ -1121,9 +1136,11 @@ __device__ inline void batch_compact(const BatchParams& bp) {
     nact += __popc(m);
     units += __shfl_sync(0xffffffffu, x, 31);
   }
+  for (int o = 16; o > 0; o >>= 1) cells += __shfl_xor_sync(0xffffffffu, cells, o);
   if (lane == 0) {
     tab->nact = nact;
     tab->units = units;
+    tab->cells = cells;
     tab->u0[nact] = units;
   }
 }
@@ -1161,6 +1178,7 @@ __global__ void __launch_bounds__(kFoldThreads) k_batch_begin(const BatchParams 
     b->stop_on_done = stop_on_done;
     const int done = nact == 0 || max_steps <= 0 || b->status != 0;
     b->done = done;
+    b->last_stamp = global_ns();
     __threadfence();
     if (bp.use_cond) cudaGraphSetConditional(bp.cond, done ? 0u : 1u);
   }
@@ -1194,6 +1212,8 @@ __global__ void __launch_bounds__(kFoldThreads) k_batch_fold(const BatchParams b
   if (*(volatile int*)&b->done) return;  // the loop ended at an earlier step
   const BatchTab* tab = bp.tab;
   const int nact = tab->nact;
+  const long long step_cells = tab->cells;  // read before any recompaction below
+  const int step_units = tab->units;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (int a = warp; a < nact; a += nwarps) {  // volume sums of the reporting scenarios
     const BatchScen* s = &bp.scen[tab->act[a]];
@@ -1232,6 +1252,18 @@ __global__ void __launch_bounds__(kFoldThreads) k_batch_fold(const BatchParams b
                       *(volatile int*)&b->status != 0 || (b->stop_on_done && b->completed > 0) ||
                       attn;
     b->done = stop;
+    if (b->trace != nullptr) {
+      const long long k = step_new - 1 - b->trace_base;
+      const unsigned long long now = global_ns();
+      if (k >= 0 && k < b->trace_cap) {
+        unsigned long long* r = b->trace + 4 * k;
+        r[0] = b->last_stamp;
+        r[1] = now;
+        r[2] = (unsigned long long)step_cells;
+        r[3] = (unsigned long long)step_units;
+      }
+      b->last_stamp = now;
+    }
     __threadfence();
     if (bp.use_cond) cudaGraphSetConditional(bp.cond, stop ? 0u : 1u);
   }

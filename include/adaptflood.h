@@ -378,6 +378,15 @@ int af_batch_set_balance(af_batch* b, int strips_per_warp);
  * (t >= t_stop), -1 stopped on a bad state (non-finite or non-positive dt). */
 int af_batch_slot_status(const af_batch* b, int slot, double* t, double* dt_last, double* hmax,
                          int64_t* steps, int* state);
+/* Per-step trace of a batch (no counterpart in the reference: it runs one
+ * grid per process).  af_batch_set_trace(b, cap) (re)starts it with room for
+ * cap batch steps (0 stops it); af_batch_get_trace copies up to cap records
+ * of the steps since then, four int64 each: the step's start and end on the
+ * device clock (ns) and the cells and strips it stepped; *n gets how many
+ * there are.  Neither may be called while a launch is in flight. */
+int af_batch_set_trace(af_batch* b, int64_t cap);
+int af_batch_get_trace(af_batch* b, int64_t* rec, int64_t cap, int64_t* n);
+
 /* State of a slot in the reference layout, HOST FP64 arrays (as
  * af_sim_get_state); any pointer may be NULL. */
 int af_batch_get_state(af_batch* b, int slot, double* H, double* Qx, double* Qy);

@@ -225,3 +225,20 @@ def test_batch_step_limits_are_exact(cuda):
             total += n
             assert b.info()["batch_steps"] == total
             assert all(b.status(s)[3] == total for s in slots)
+
+
+def test_batch_trace_records_every_step(cuda):
+    cases = _cases()[:3]
+    with Batch("f32", arena_bytes=ARENA) as b:
+        slots = [b.add(c) for c in cases]
+        b.set_trace(100000)
+        n = b.run()
+        rec = b.trace()
+        steps = [b.status(s)[3] for s in slots]
+    assert rec.shape == (n, 4) and n == max(steps)
+    start, end, cells, units = rec.T
+    assert np.all(end >= start) and np.all(start[1:] >= end[:-1])
+    # every member is active until it has taken its own steps
+    want = [sum(c.cells for c, k in zip(cases, steps) if k > i) for i in range(n)]
+    np.testing.assert_array_equal(cells, want)
+    assert np.all(units > 0)
