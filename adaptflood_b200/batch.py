@@ -241,3 +241,30 @@ class Arena:
         _lib.check(self.lib.af_arena_stats(self.h, C.byref(u), C.byref(lf), C.byref(b)),
                    "af_arena_stats")
         return u.value, lf.value, b.value
+
+
+def trace_summary(rec: np.ndarray, bytes_per_cell: float, peak_gbs: float) -> dict:
+    """Where a traced batch run spent its time: steps grouped by the cells
+    they stepped (powers of four), each group's share of the time and of the
+    cell-updates, and its HBM rate (algorithmic bytes / device time)."""
+    if rec.size == 0:
+        return {}
+    start, end, cells, _units = (rec[:, k].astype(np.float64) for k in range(4))
+    dt = (end - start) * 1e-9
+    total = float(dt.sum())
+    cu = float(cells.sum())
+    edges = [0.0] + [float(4 ** k) for k in range(8, 15)] + [np.inf]
+    groups = []
+    for lo, hi in zip(edges[:-1], edges[1:]):
+        m = (cells >= lo) & (cells < hi)
+        if not m.any():
+            continue
+        t = float(dt[m].sum())
+        c = float(cells[m].sum())
+        groups.append({"cells": [lo, hi if np.isfinite(hi) else None], "steps": int(m.sum()),
+                       "time_share": t / total, "cell_update_share": c / cu,
+                       "hbm_frac": (c * bytes_per_cell / t / 1e9) / peak_gbs if t > 0 else None,
+                       "us_per_step": t / int(m.sum()) * 1e6})
+    return {"steps": int(rec.shape[0]), "seconds": total,
+            "min_step_us": float(dt.min() * 1e6), "groups": groups}
+

@@ -303,7 +303,7 @@ def run_ensemble(args, device, peak):
     beside it a sample of the same scenarios on the plain FP64 single-grid
     path, one at a time."""
     import torch
-    from adaptflood_b200.batch import Batch, size_class
+    from adaptflood_b200.batch import Batch, size_class, trace_summary
     from adaptflood_b200.sim import Simulation
     from adaptflood_b200.tune import tune_rows
     cases = sc.config4(count=args.ensemble)
@@ -315,6 +315,7 @@ def run_ensemble(args, device, peak):
     with Batch("f32", device=device, rows=rows) as b:
         need = sum(b.footprint(c, f) for c, f in zip(cases, forcings))
         slots = [b.add(c, f) for c, f in zip(cases, forcings)]
+        b.set_trace(1 << 17)
         stream, e0, e1 = _event_timer(b.stream, device)
         torch.cuda.synchronize(device)
         e0.record(stream)
@@ -324,6 +325,7 @@ def run_ensemble(args, device, peak):
         ms = e0.elapsed_time(e1)
         steps = [b.status(s)[3] for s in slots]
         batch_steps = b.info()["batch_steps"]
+        trace = b.trace()
     cu = sum(c.cells * n for c, n in zip(cases, steps))
     value = cu / (ms / 1e3)
     ach = BYTES_PER_CELL["f32"] * value / 1e9
@@ -357,6 +359,7 @@ def run_ensemble(args, device, peak):
                      "frac": ach / peak, "algorithmic_bytes_per_cell": BYTES_PER_CELL["f32"],
                      "note": "whole batch loop (graph launch incl. begin kernel and the tail "
                              "where few scenarios remain) / wall time on the device"},
+        "trace": trace_summary(trace, BYTES_PER_CELL["f32"], peak),
         "tuned_rows": {str(k): v for k, v in rows.items()}, "tune_seconds": tune_s,
         "plain_fp64": {"value": v64, "unit": "cell-updates/s", "scenarios": len(pick),
                        "path": "Simulation f64, one scenario at a time, CUDA events around "
