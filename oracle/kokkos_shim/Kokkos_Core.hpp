@@ -15,6 +15,12 @@
 //   fence(), initialize(), finalize(), DefaultExecutionSpace, KOKKOS_LAMBDA,
 //   KOKKOS_INLINE_FUNCTION, atomic_add, atomic_min.
 //
+// AF_SHIM_MANAGED: views in CudaUVMSpace are allocated with
+// cudaMallocManaged, as Kokkos' CUDA backend does for that space, so the
+// reference's main.cpp can be linked against a GPU implementation of
+// src/kernels.hpp (the drop-in binding) while its inline loops keep touching
+// the same arrays on the host.  Without it every view lives in host memory.
+//
 // Determinism notes:
 //   * Max reductions are order independent, so FindHmax is exact.
 //   * Sum reductions use a fixed static partition by thread id and combine the
@@ -35,6 +41,11 @@
 #include <typeinfo>
 #include <vector>
 #include <omp.h>
+#ifdef AF_SHIM_MANAGED
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstdlib>
+#endif
 
 #define KOKKOS_LAMBDA [=]
 #define KOKKOS_INLINE_FUNCTION inline
@@ -59,6 +70,32 @@ constexpr long kSerialBelow = 256;
 template <class DataType, class Space = HostSpace>
 class View;
 
+// Storage of a view: host memory, or managed memory for CudaUVMSpace in the
+// AF_SHIM_MANAGED build.  Zero-filled, as Kokkos value-initialises views.
+template <class T, class Space>
+struct ViewStore {
+  std::vector<T> v;
+  explicit ViewStore(size_t n) : v(n, T()) {}
+  T* data() { return v.data(); }
+};
+#ifdef AF_SHIM_MANAGED
+template <class T>
+struct ViewStore<T, CudaUVMSpace> {
+  T* p = nullptr;
+  explicit ViewStore(size_t n) {
+    if (cudaMallocManaged(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess) {
+      std::fprintf(stderr, "cudaMallocManaged of %zu bytes failed\n", n * sizeof(T));
+      std::abort();
+    }
+    std::memset(p, 0, n * sizeof(T));
+  }
+  ~ViewStore() { cudaFree(p); }
+  ViewStore(const ViewStore&) = delete;
+  ViewStore& operator=(const ViewStore&) = delete;
+  T* data() { return p; }
+};
+#endif
+
 // Rank-1 view with shared (reference-counted) storage, so copies made by
 // by-value lambda capture alias the same buffer, as Kokkos views do.
 template <class T, class Space>
@@ -69,7 +106,7 @@ class View<T*, Space> {
 
   View() = default;
   View(const std::string& label, size_t n)
-      : label_(label), store_(std::make_shared<std::vector<T>>(n, T())), n_(n) {
+      : label_(label), store_(std::make_shared<ViewStore<T, Space>>(n)), n_(n) {
     ptr_ = store_->data();
   }
 
@@ -82,7 +119,7 @@ class View<T*, Space> {
 
  private:
   std::string label_;
-  std::shared_ptr<std::vector<T>> store_;
+  std::shared_ptr<ViewStore<T, Space>> store_;
   T* ptr_ = nullptr;
   size_t n_ = 0;
 };
