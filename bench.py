@@ -78,6 +78,14 @@ def parse():
                     help="Poisson arrival rates (req/s) of the serving leg")
     ap.add_argument("--fp64-sample", type=int, default=12,
                     help="ensemble scenarios run one at a time on the plain FP64 path")
+    ap.add_argument("--table", action="store_true",
+                    help="measure every configuration (C1-C5: GPU FP32 and FP64, the "
+                         "reference's CPU code) and print one JSON object instead of the "
+                         "benchmark line")
+    ap.add_argument("--largest", type=int, default=16384,
+                    help="grid size of the largest-configuration leg (C3; 0 = skip)")
+    ap.add_argument("--largest-steps", type=int, default=40,
+                    help="timed steps of each precision in the largest-configuration leg")
     return ap.parse_args()
 
 
@@ -156,17 +164,20 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_reference(case, forcing, h0, seconds: float, max_steps: int):
+def cpu_reference(case, forcing, h0, seconds: float, max_steps: int, start: float = T_START,
+                  warmup: int = 1):
     """The reference's own code (oracle/_ref) on this host's cores: as many
-    steps of the same workload as fit in `seconds` (after one warm-up step)."""
+    steps of the same workload as fit in `seconds` (after `warmup` untimed
+    steps)."""
     from oracle import oracle as orc
     if not orc.ref_available():
         return None
     r = orc.RefSim.from_case(case, forcing)
-    F = (case.nx + 1) * (case.ny + 1)
-    z = np.zeros(F)
-    r.set_state(h0.ravel(), z, z, T_START)
-    r.run(1e30, max_steps=1)
+    if start != 0.0:
+        F = (case.nx + 1) * (case.ny + 1)
+        z = np.zeros(F)
+        r.set_state(h0.ravel(), z, z, start)
+    r.run(1e30, max_steps=max(1, warmup))
     n = 0
     t0 = time.perf_counter()
     while n < max_steps:
@@ -180,7 +191,9 @@ def cpu_reference(case, forcing, h0, seconds: float, max_steps: int):
             "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
             "kind": "reference", "steps": n, "seconds": el,
             "sample": f"{n} steps of the same {case.nx}x{case.ny} workload from the same start "
-                      f"state (after 1 warm-up step), reference src/kernels.cpp + main.cpp loop "
+                      f"state at t={start:g}s (after {max(1, warmup)} warm-up steps), reference "
+                      f"src/kernels.cpp "
+                      f"+ main.cpp loop "
                       f"compiled -O3 -fopenmp against the Kokkos-API shim"}
 
 
@@ -189,14 +202,14 @@ def run_reference(args, rank: int, world: int):
         return
     case, forcing = workload(args.size)
     res = cpu_reference(case, forcing, case.h0, seconds=max(30.0, args.cpu_seconds),
-                        max_steps=max(1, args.steps))
+                        max_steps=max(1, args.steps), warmup=args.warmup)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built here"}))
         return
     ms = res["seconds"] * 1e3 / res["steps"]
     print(json.dumps({
         "impl": "reference", "metric": "cell-updates/s", "value": res["value"],
-        "unit": "cell-updates/s", "n_gpus": 0, "steps": res["steps"], "warmup": 1,
+        "unit": "cell-updates/s", "n_gpus": 0, "steps": res["steps"], "warmup": max(1, args.warmup),
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "config": describe(args.size),
         "cpu_baseline": {"value": res["value"], "unit": "cell-updates/s", "cores": res["cores"],
@@ -205,14 +218,15 @@ def run_reference(args, rank: int, world: int):
                 "d2h_bytes_per_step": 0}}))
 
 
-def time_fused(case, forcing, precision, steps, warmup, device, dist=None):
+def time_fused(case, forcing, precision, steps, warmup, device, dist=None, start=T_START):
     """K fused steps as one graph launch, CUDA events on the sim's stream."""
     import torch
     from adaptflood_b200.sim import Simulation
-    F = (case.nx + 1) * (case.ny + 1)
-    zero = np.zeros(F)
     s = Simulation(case, precision, device=device, forcing=forcing)
-    s.set_state(case.h0, zero, zero, T_START)
+    if start != 0.0:
+        F = (case.nx + 1) * (case.ny + 1)
+        zero = np.zeros(F)
+        s.set_state(case.h0, zero, zero, start)
     s.run(1e30, max_steps=warmup)
     stream = torch.cuda.ExternalStream(s.stream, device=device)
     e0 = torch.cuda.Event(enable_timing=True)
@@ -403,6 +417,134 @@ def run_serving(args, device):
     return out
 
 
+def run_largest(args, device, peak):
+    """C3, the largest single-GPU configuration: 16384^2 at 2 m with Gaussian
+    ponds and a 1 m deep 512^2 reservoir, from its own start state (t = 0),
+    K steps of the fused step in FP32 and in FP64 (CUDA events on the
+    simulation's stream), each with its HBM roofline, and the reference's CPU
+    code on a bounded sample of the same steps."""
+    n = args.largest
+    case = sc.config3(n=n)
+    forcing = fc.pack(case)
+    out = {"workload": f"C3 mixed-precision stress {n}x{n} dx=2m, Gaussian ponds, 1 m deep "
+                       f"512x512 reservoir, from t=0", "cells": case.cells,
+           "steps": args.largest_steps}
+    for prec in ("f32", "f64"):
+        ms, info = time_fused(case, forcing, prec, args.largest_steps, max(3, args.warmup),
+                              device, start=0.0)
+        v = case.cells * args.largest_steps / (ms / 1e3)
+        ach = BYTES_PER_CELL[prec] * v / 1e9
+        out[prec] = {"value": v, "unit": "cell-updates/s", "ms_per_step": ms / args.largest_steps,
+                     "roofline": {"achieved": ach, "peak": peak, "frac": ach / peak,
+                                  "unit": "GB/s",
+                                  "algorithmic_bytes_per_cell": BYTES_PER_CELL[prec]},
+                     "state_after": info}
+    if not args.no_cpu_baseline:
+        cpu = cpu_reference(case, forcing, case.h0, args.cpu_seconds / 2, 20, start=0.0)
+        if cpu is not None:
+            out["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind",
+                                                       "sample")}
+    return out
+
+
+def _full_run(case, forcing, precision, device):
+    """One whole run on the fused path from t = 0 to sim_time, timed with
+    CUDA events on the simulation's stream; (cell-updates/s, steps)."""
+    import torch
+    from adaptflood_b200.sim import Simulation
+    with Simulation(case, precision, device=device, forcing=forcing) as s:
+        st, a0, a1 = _event_timer(s.stream, device)
+        torch.cuda.synchronize(device)
+        a0.record(st)
+        s.launch(case.sim_time)
+        a1.record(st)
+        s.sync()
+        ms = a0.elapsed_time(a1)
+        n = s.steps
+    return case.cells * n / (ms / 1e3), n
+
+
+def _cpu_full_run(case, forcing):
+    """The reference's own code from t = 0 to sim_time on all host cores."""
+    from oracle import oracle as orc
+    r = orc.RefSim.from_case(case, forcing)
+    t0 = time.perf_counter()
+    n = r.run(case.sim_time)
+    el = time.perf_counter() - t0
+    r.close()
+    return case.cells * n / el, n, el
+
+
+def run_table(args):
+    """Every configuration, GPU FP32 / FP64 and the reference's CPU code, for
+    the result table of the baseline document (one JSON object)."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    peak, peak_kind = measured_peak()
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    rows = {"peak_gbs": peak, "peak_source": peak_kind, "cpu_cores": cores}
+    # C1: whole runs (L2-resident state: launch- and latency-bound)
+    c1 = sc.config1()
+    f1 = fc.pack(c1)
+    v64, n64 = _full_run(c1, f1, "f64", local)
+    v32, n32 = _full_run(c1, f1, "f32", local)
+    vc, nc, el = _cpu_full_run(c1, f1)
+    rows["C1"] = {"gpu_f64": v64, "gpu_f32": v32, "steps_f64": n64, "steps_f32": n32,
+                  "cpu": vc, "cpu_steps": nc, "cpu_seconds": el,
+                  "hbm_frac_f32": BYTES_PER_CELL["f32"] * v32 / 1e9 / peak,
+                  "hbm_frac_f64": BYTES_PER_CELL["f64"] * v64 / 1e9 / peak}
+    # C2: the benchmark's flooded start, K steps; CPU: 200 steps
+    case, forcing = workload(8192)
+    r = {}
+    for prec in ("f32", "f64"):
+        ms, _ = time_fused(case, forcing, prec, args.steps, args.warmup, local)
+        r["gpu_" + prec] = case.cells * args.steps / (ms / 1e3)
+        r["hbm_frac_" + prec] = BYTES_PER_CELL[prec] * r["gpu_" + prec] / 1e9 / peak
+    cpu = cpu_reference(case, forcing, case.h0, 1e9, 200)
+    r["cpu"], r["cpu_sample"] = cpu["value"], cpu["sample"]
+    rows["C2"] = r
+    del case, forcing
+    # C3: from its own start, K steps; CPU: 100 steps
+    args.largest = 16384
+    args.largest_steps = max(args.largest_steps, 40)
+    args.no_cpu_baseline = True
+    big = run_largest(args, local, peak)
+    c3, f3 = sc.config3(), None
+    f3 = fc.pack(c3)
+    cpu = cpu_reference(c3, f3, c3.h0, 1e9, 100, start=0.0)
+    rows["C3"] = {"gpu_f32": big["f32"]["value"], "gpu_f64": big["f64"]["value"],
+                  "hbm_frac_f32": big["f32"]["roofline"]["frac"],
+                  "hbm_frac_f64": big["f64"]["roofline"]["frac"],
+                  "cpu": cpu["value"], "cpu_sample": cpu["sample"]}
+    del c3, f3
+    # C4: the batch, the plain FP64 sample; CPU: 8 scenarios across the size range,
+    # 50 steps each from t = 0
+    args.ensemble = 256
+    ens = run_ensemble(args, local, peak)
+    cases = sc.config4()
+    order = sorted(range(len(cases)), key=lambda k: cases[k].cells)
+    pick = [order[int(round(q * (len(order) - 1) / 7))] for q in range(8)]
+    from oracle import oracle as orc
+    cu, el = 0, 0.0
+    for k in pick:
+        ref = orc.RefSim.from_case(cases[k], fc.pack(cases[k]))
+        t0 = time.perf_counter()
+        n = ref.run(cases[k].sim_time, max_steps=50)
+        el += time.perf_counter() - t0
+        cu += cases[k].cells * n
+        ref.close()
+    rows["C4"] = {"gpu_f32_batch": ens["value"], "hbm_frac_f32": ens["roofline"]["frac"],
+                  "gpu_f64_plain": ens["plain_fp64"]["value"], "cpu": cu / el,
+                  "cpu_sample": "8 scenarios spread over the size range, 50 steps each from "
+                                "t=0", "scenarios_per_s": ens["scenarios_per_s"],
+                  "trace": ens.get("trace")}
+    # C5: serving
+    args.serve_requests = max(args.serve_requests, 32)
+    rows["C5"] = run_serving(args, local)
+    print(json.dumps(rows))
+
+
 def traffic_per_cell(kernel_key: str):
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
@@ -471,7 +613,9 @@ def run_ours(args, rank: int, world: int):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference(case, forcing, case.h0, args.cpu_seconds, 10_000)
-    ens = serve = None
+    ens = serve = big = None
+    if world == 1 and args.largest > 0:
+        big = run_largest(args, local, peak)
     if world == 1 and args.ensemble > 0:
         ens = run_ensemble(args, local, peak)
     if world == 1 and args.serve_requests > 0:
@@ -487,7 +631,14 @@ def run_ours(args, rank: int, world: int):
                          "frac": ach32 / peak, "peak_source": peak_kind,
                          "algorithmic_bytes_per_cell": BYTES_PER_CELL["f32"],
                          "traffic": None if tr32 is None else tr32 * cells,
-                         "kernel": "k_step<float> (fused step)"},
+                         "kernel": "k_step<float> (fused step)",
+                         # the same step in FP64 (the plain form, like-for-like with the
+                         # FP64 reference arm) on the same workload
+                         "fp64": {"value": value64, "ms_per_step": step_ms64,
+                                  "achieved": ach64, "frac": ach64 / peak,
+                                  "algorithmic_bytes_per_cell": BYTES_PER_CELL["f64"],
+                                  "traffic": None if tr64 is None else tr64 * cells,
+                                  "kernel": "k_step<double> (fused step)"}},
             "fp64": {"value": value64, "ms_per_step": step_ms64, "dtype": "f64",
                      "roofline": {"achieved": ach64, "peak": peak, "frac": ach64 / peak,
                                   "unit": "GB/s",
@@ -508,6 +659,12 @@ def run_ours(args, rank: int, world: int):
         }
         if cpu is not None:
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        if big is not None:
+            line["largest"] = big
+            line["roofline"]["largest_config"] = {
+                "workload": big["workload"],
+                "f32": {"value": big["f32"]["value"], "frac": big["f32"]["roofline"]["frac"]},
+                "f64": {"value": big["f64"]["value"], "frac": big["f64"]["roofline"]["frac"]}}
         if ens is not None:
             line["ensemble"] = ens
         if serve is not None:
@@ -524,6 +681,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.table:
+        run_table(args)
     else:
         run_ours(args, rank, world)
 
