@@ -7,7 +7,16 @@ initial state to the case's sim_time on the device, and reports
 * max and RMS depth error of the FP32 run against the FP64 run (m);
 * relative mass error: |V32 - V64| / V64 of the end volumes, and the largest
   such error over the mass reports along the run (FP64-accumulated volumes);
-* step counts, end times and rates of both runs.
+* step counts, end times and rates of both runs;
+* with --input-rounding, the same errors of a third run: FP64 arithmetic on
+  the DEM and start depth rounded to FP32 (the inputs an FP32 state holds),
+  against plain FP64 -- how much of the FP32 run's error the rounding of the
+  inputs alone accounts for (the conditioning of the case).
+
+--config 4 / --config 5 report per scenario over a sample of the ensemble
+(C4, run as one FP32 batch) or of the served requests (C5, served by
+continuous batching at --rate req/s): max depth error and relative mass error
+of each scenario against its own FP64 single-grid run.
 
     python -m adaptflood_b200.accuracy --config 3            # 16384^2, 10800 s
     python -m adaptflood_b200.accuracy --config 3 --size 4096 --sim-time 1800
@@ -43,6 +52,16 @@ def make_case(config: int, size=None, sim_time=None) -> sc.Case:
     return case
 
 
+def rounded_inputs(case: sc.Case) -> sc.Case:
+    """The case with its DEM and start depth rounded to FP32 (held as FP64)."""
+    import copy
+    c = copy.copy(case)
+    c.dem = case.dem.astype(np.float32).astype(np.float64)
+    if case.h0 is not None:
+        c.h0 = case.h0.astype(np.float32).astype(np.float64)
+    return c
+
+
 def run(case: sc.Case, precision: str, device: int = 0):
     import torch
     f = fc.pack(case)
@@ -59,28 +78,33 @@ def run(case: sc.Case, precision: str, device: int = 0):
             "mass_t": mt, "mass_v": mv}
 
 
-def report(case: sc.Case, device: int = 0) -> dict:
-    r64 = run(case, "f64", device)
-    r32 = run(case, "f32", device)
-    d = r32["H"] - r64["H"]
+def compare(case: sc.Case, r: dict, r64: dict) -> dict:
+    """Depth and mass errors of run r against the FP64 run r64."""
     valid = case.dem != case.nodata
-    err = np.abs(d[valid])
-    k = min(len(r32["mass_v"]), len(r64["mass_v"]))
+    err = np.abs((r["H"] - r64["H"])[valid])
+    k = min(len(r["mass_v"]), len(r64["mass_v"]))
     # mass reports fall at the first step with t >= each report time; the two
     # runs' dt differ slightly, so compare the reports pairwise by index
-    rel_series = (np.abs(r32["mass_v"][:k] - r64["mass_v"][:k]) /
+    rel_series = (np.abs(r["mass_v"][:k] - r64["mass_v"][:k]) /
                   np.maximum(np.abs(r64["mass_v"][:k]), 1e-300)) if k else np.zeros(1)
+    return {"max_depth_error_m": float(err.max()) if err.size else 0.0,
+            "rms_depth_error_m": float(np.sqrt(np.mean(err ** 2))) if err.size else 0.0,
+            "relative_mass_error_end": abs(r["vol"] - r64["vol"]) / max(abs(r64["vol"]), 1e-300),
+            "relative_mass_error_max_over_reports": float(rel_series.max()) if k else None,
+            "mass_reports_compared": int(k)}
+
+
+def report(case: sc.Case, device: int = 0, input_rounding: bool = False) -> dict:
+    r64 = run(case, "f64", device)
+    r32 = run(case, "f32", device)
+    c32 = compare(case, r32, r64)
     cells = case.cells
-    return {
+    out = {
         "case": case.name, "nx": case.nx, "ny": case.ny, "dx": case.dx,
         "sim_time": case.sim_time,
-        "max_depth_error_m": float(err.max()) if err.size else 0.0,
-        "rms_depth_error_m": float(np.sqrt(np.mean(err ** 2))) if err.size else 0.0,
+        **c32,
         "max_depth_m": float(r64["H"].max()),
         "wet_cells_fp64": int(np.count_nonzero(r64["H"] > 0.001)),
-        "relative_mass_error_end": abs(r32["vol"] - r64["vol"]) / abs(r64["vol"]),
-        "relative_mass_error_max_over_reports": float(rel_series.max()) if k else None,
-        "mass_reports_compared": int(k),
         "volume_fp64_m3": r64["vol"], "volume_fp32_m3": r32["vol"],
         "steps": {"f64": r64["steps"], "f32": r32["steps"]},
         "t_end": {"f64": r64["t_end"], "f32": r32["t_end"]},
@@ -89,6 +113,71 @@ def report(case: sc.Case, device: int = 0) -> dict:
         "seconds": {"f64": r64["seconds"], "f32": r32["seconds"]},
         "tolerance": {"max_depth_error_m": 1e-3, "relative_mass_error": 1e-6},
     }
+    if input_rounding:
+        rr = run(rounded_inputs(case), "f64", device)
+        out["fp64_on_fp32_rounded_inputs"] = dict(compare(case, rr, r64), volume_m3=rr["vol"],
+                                                  steps=rr["steps"])
+    return out
+
+
+def _scenario_errors(cases, results32, device):
+    """Per scenario: the FP32 result (depth field, end volume) against the
+    scenario's own FP64 single-grid run."""
+    rows = []
+    for case, (H32, vol32) in zip(cases, results32):
+        r64 = run(case, "f64", device)
+        valid = case.dem != case.nodata
+        err = np.abs((H32 - r64["H"])[valid])
+        rows.append({"name": case.name, "cells": case.cells, "dx": case.dx,
+                     "max_depth_error_m": float(err.max()) if err.size else 0.0,
+                     "relative_mass_error_end": abs(vol32 - r64["vol"]) /
+                     max(abs(r64["vol"]), 1e-300)})
+    md = [r["max_depth_error_m"] for r in rows]
+    mm = [r["relative_mass_error_end"] for r in rows]
+    return {"scenarios": len(rows), "max_depth_error_m": max(md),
+            "median_max_depth_error_m": float(np.median(md)),
+            "relative_mass_error_max": max(mm), "relative_mass_error_median": float(np.median(mm)),
+            "per_scenario": rows,
+            "tolerance": {"max_depth_error_m": 1e-3, "relative_mass_error": 1e-6}}
+
+
+def ensemble_report(count: int = 16, device: int = 0) -> dict:
+    """C4: a sample spread over the ensemble's size range, run as one FP32
+    batch, each member against its FP64 single-grid run."""
+    from .batch import Batch
+    cases = sc.config4()
+    order = sorted(range(len(cases)), key=lambda k: cases[k].cells)
+    pick = [cases[order[int(round(q * (len(order) - 1) / max(1, count - 1)))]]
+            for q in range(count)]
+    with Batch("f32", device=device) as b:
+        slots = [b.add(c, fc.pack(c)) for c in pick]
+        b.run()
+        res = []
+        for c, sl in zip(pick, slots):
+            H = b.depth(sl)
+            res.append((H, float(np.sum(H) * c.dx * c.dx)))
+    out = _scenario_errors(pick, res, device)
+    out["workload"] = f"C4 sample of {count} scenarios across the size range, one FP32 batch"
+    return out
+
+
+def served_report(count: int = 32, rate: float = 50.0, device: int = 0) -> dict:
+    """C5: the served requests (continuous batching at `rate` req/s), each
+    result against the request's FP64 single-grid run."""
+    from .serve import Request, Server, poisson_arrivals
+    cases = sc.config5(count=count)
+    rng = np.random.default_rng(int(rate * 1000) + 7)
+    arr = poisson_arrivals(rate, len(cases), rng)
+    reqs = [Request(k, float(arr[k]), cases[k], fc.pack(cases[k])) for k in range(len(cases))]
+    with Server("f32", device=device, keep_results=True) as srv:
+        srv.run(reqs)
+    res = []
+    for c, r in zip(cases, reqs):
+        H = r.result
+        res.append((H, float(np.sum(H) * c.dx * c.dx)))
+    out = _scenario_errors(cases, res, device)
+    out["workload"] = f"C5: {count} requests served by continuous batching at {rate} req/s"
+    return out
 
 
 def main():
@@ -97,9 +186,18 @@ def main():
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--sim-time", type=float, default=None)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--input-rounding", action="store_true",
+                    help="also run FP64 on the FP32-rounded DEM and start depth")
+    ap.add_argument("--count", type=int, default=None, help="scenarios (configs 4 and 5)")
+    ap.add_argument("--rate", type=float, default=50.0, help="arrival rate (config 5)")
     a = ap.parse_args()
-    case = make_case(a.config, a.size, a.sim_time)
-    print(json.dumps(report(case, a.device)))
+    if a.config == 4:
+        print(json.dumps(ensemble_report(a.count or 16, a.device)))
+    elif a.config == 5:
+        print(json.dumps(served_report(a.count or 32, a.rate, a.device)))
+    else:
+        case = make_case(a.config, a.size, a.sim_time)
+        print(json.dumps(report(case, a.device, a.input_rounding)))
 
 
 if __name__ == "__main__":
