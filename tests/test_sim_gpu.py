@@ -195,9 +195,9 @@ def test_loaded_par_runs_like_generated_case(cuda, tmp_path):
     (250, 203, 22, dict(free=(1, 0, 1, 1), nodata_block=True, n_hvar=2)),
 ])
 def test_fused_equals_dropin_kernels_bitwise(cuda, nx, ny, seed, kw):
-    """Both GPU paths use CUDA's pow, so the fused kernel -- if it keeps the
-    reference's operation order everywhere -- must equal the drop-in
-    per-function kernels bit for bit, step after step."""
+    """Both GPU paths use the same pow (af_pow.cuh), so the fused kernel -- if
+    it keeps the reference's operation order everywhere -- must equal the
+    drop-in per-function kernels bit for bit, step after step."""
     import torch
     from adaptflood_b200 import kernels as K
     case = _strip_edge_case(nx, ny, seed, sim_time=150.0, **kw)
