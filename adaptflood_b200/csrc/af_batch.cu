@@ -440,6 +440,28 @@ static int add(Batch& b, const af_case_desc* c, const af_forcing_desc* f, const 
   p.ef = c->east_free;
   p.nf = c->north_free;
   p.sf = c->south_free;
+  {
+    // Whether the stored DEM has a nodata cell (the first word of the
+    // scenario's strip partials, unused until it is stepped, as the flag).
+    int* flag = (int*)(base + L.partials);
+    const unsigned gn = grid_for((long long)L.nx * L.ny, 256, 8);
+    cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), b.cst);
+    if (e == cudaSuccess) {
+      if (b.prec == AF_PREC_F64)
+        k_any_nodata<double><<<gn, 256, 0, b.cst>>>((const double*)p.DEM, L.nx, L.ny, L.P,
+                                                    c->nodata, flag);
+      else
+        k_any_nodata<float><<<gn, 256, 0, b.cst>>>((const float*)p.DEM, L.nx, L.ny, L.P,
+                                                   c->nodata, flag);
+      e = cudaGetLastError();
+    }
+    int hflag = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost,
+                                              b.cst);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b.cst);
+    if (e != cudaSuccess) return fail(cuda_fail(e));
+    p.has_nodata = hflag;
+  }
   p.src_type = (const int*)(base + L.src_type);
   p.src_value = (const double*)(base + L.src_value);
   p.src_off = (const int*)(base + L.src_off);

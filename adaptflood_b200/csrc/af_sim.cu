@@ -399,6 +399,26 @@ static int refresh_hmax(Sim& s, int parity) {
   return AF_OK;
 }
 
+// Whether the stored DEM has a nodata cell (one word of the partials buffer,
+// which holds nothing between launches, as the flag).
+static int any_nodata(Sim& s, int* out) {
+  int* flag = static_cast<int*>(s.partials.p);
+  AF_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s.st));
+  const unsigned grid = grid_for((long long)s.c.nx * s.c.ny, 256, 8);
+  if (s.prec == AF_PREC_F64)
+    k_any_nodata<double><<<grid, 256, 0, s.st>>>(s.buf<double>(s.DEM), s.c.nx, s.c.ny, s.P,
+                                                 s.c.nodata, flag);
+  else
+    k_any_nodata<float><<<grid, 256, 0, s.st>>>(s.buf<float>(s.DEM), s.c.nx, s.c.ny, s.P,
+                                                s.c.nodata, flag);
+  AF_CUDA(cudaGetLastError());
+  int h = 0;
+  AF_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, s.st));
+  AF_CUDA(cudaStreamSynchronize(s.st));
+  *out = h;
+  return AF_OK;
+}
+
 static int read_ctl(Sim& s) {
   AF_CUDA(cudaMemcpyAsync(s.pinned_ctl, s.ctl.p, sizeof(SimCtl), cudaMemcpyDeviceToHost, s.st));
   AF_CUDA(cudaStreamSynchronize(s.st));
@@ -641,6 +661,7 @@ static int create(const af_case_desc* c, const af_forcing_desc* f, const double*
   p.ef = c->east_free;
   p.nf = c->north_free;
   p.sf = c->south_free;
+  AF_TRY(any_nodata(*s, &p.has_nodata));
   p.src_type = (const int*)s->src_type.p;
   p.src_value = (const double*)s->src_value.p;
   p.src_off = (const int*)s->src_off.p;

@@ -87,6 +87,21 @@ __global__ void k_hmax_int(const T* __restrict__ H, const T* __restrict__ Z, int
   if ((threadIdx.x & 31) == 0 && m > -DBL_MAX) atomicMax(acc, ord_encode(m));
 }
 
+// Sets *flag when some cell of the stored DEM (state precision) equals nodata.
+template <typename T>
+__global__ void k_any_nodata(const T* __restrict__ Z, int nx, int ny, int P, double nodata,
+                             int* flag) {
+  const T nd = T(nodata);
+  const long long n = (long long)nx * ny;
+  bool hit = false;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const long long j = k / nx, i = k - j * nx;
+    hit |= Z[j * P + i] == nd;
+  }
+  if (__any_sync(0xffffffffu, hit) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
 static __global__ void k_ctl_fold_hmax(SimCtl* ctl) {
   ctl->hmax = ord_decode(ctl->hmax_acc);
   ctl->hmax_acc = ord_encode(-DBL_MAX);

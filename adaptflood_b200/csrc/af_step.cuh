@@ -77,6 +77,7 @@ struct StepParams {
   double dx, dxinv, dA, fpn, depth_thresh, max_hflow, g, cfl, init_tstep, nodata;
   double mass_int;
   int wf, ef, nf, sf;
+  int has_nodata;  // some DEM cell (as stored) equals nodata; 0 lets FP32 skip the tests
   // point sources, sorted by cell (file order within a cell)
   const int* src_type;
   const double* src_value;
@@ -238,6 +239,7 @@ __device__ inline T bc_depth(int b, SeriesTable tb, double t) {
 
 // FP64: the reference's expressions exactly (src/kernels.cpp:60-84), with the
 // C library's pow algorithm (af_pow.cuh).
+template <bool ND>  // FP64 keeps every test of the reference
 __device__ inline void row_faces(const double (&h)[2], const double (&z)[2], const double (&hN)[2],
                                  const double (&zN)[2], const double (&qxo)[2],
                                  const double (&qxoN)[2], const double (&qyo)[2],
@@ -296,6 +298,9 @@ __device__ inline void row_faces(const double (&h)[2], const double (&z)[2], con
 // hflow^(-7/3) = exp2(-7/3 * log2(hflow)) on the special-function unit.
 __device__ inline float2 f2(float a, float b) { return make_float2(a, b); }
 
+// ND: the grid has nodata cells, so a face touching one is dry; without ND
+// every cell is valid and the tests are skipped (the same results).
+template <bool ND>
 __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float2 q0, float2 qa,
                                float2 qb, float2 qc, float2 qd, bool enable,
                                const Phys<float>& ph, bool& any) {
@@ -315,8 +320,10 @@ __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float
   // way, whose values are discarded, so it is not applied.  The wet test is on
   // the unclamped depth, so a NaN depth stays dry as in the reference.
   const float2 hf = f2(fminf(hfx.x, ph.max_hflow), fminf(hfx.y, ph.max_hflow));
-  const bool wx = enable && z0.x != ph.nodata && z1.x != ph.nodata && hfx.x > ph.depth_thresh;
-  const bool wy = enable && z0.y != ph.nodata && z1.y != ph.nodata && hfx.y > ph.depth_thresh;
+  const bool vx = !ND || (z0.x != ph.nodata && z1.x != ph.nodata);
+  const bool vy = !ND || (z0.y != ph.nodata && z1.y != ph.nodata);
+  const bool wx = enable && vx && hfx.x > ph.depth_thresh;
+  const bool wy = enable && vy && hfx.y > ph.depth_thresh;
   any |= wx | wy;
   // In units of the stored Q (= Qold*dx): the reference's
   //   Q = (Qold - g*dt*hflow*Sf) / (1 + g*dt*n^2*|Qvect|/hflow^(10/3)) * dx
@@ -332,6 +339,7 @@ __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float
   return f2(wx ? __fdividef(num.x, den.x) : 0.0f, wy ? __fdividef(num.y, den.y) : 0.0f);
 }
 
+template <bool ND>
 __device__ inline void row_faces(const float (&h)[4], const float (&z)[4], const float (&hN)[4],
                                  const float (&zN)[4], const float (&qxo)[4],
                                  const float (&qxoN)[4], const float (&qyo)[4],
@@ -340,17 +348,17 @@ __device__ inline void row_faces(const float (&h)[4], const float (&z)[4], const
                                  const Phys<float>& ph, float (&qw)[4], float (&qs)[4]) {
   bool any = false;
   // west faces: (cell k-1, cell k) for k = 0..3
-  const float2 w01 = flux2(f2(zL, z[0]), f2(hL, h[0]), f2(z[0], z[1]), f2(h[0], h[1]),
+  const float2 w01 = flux2<ND>(f2(zL, z[0]), f2(hL, h[0]), f2(z[0], z[1]), f2(h[0], h[1]),
                            f2(qxo[0], qxo[1]), f2(qyoL, qyo[0]), f2(qyo[0], qyo[1]),
                            f2(qyoNL, qyoN[0]), f2(qyoN[0], qyoN[1]), true, ph, any);
-  const float2 w23 = flux2(f2(z[1], z[2]), f2(h[1], h[2]), f2(z[2], z[3]), f2(h[2], h[3]),
+  const float2 w23 = flux2<ND>(f2(z[1], z[2]), f2(h[1], h[2]), f2(z[2], z[3]), f2(h[2], h[3]),
                            f2(qxo[2], qxo[3]), f2(qyo[1], qyo[2]), f2(qyo[2], qyo[3]),
                            f2(qyoN[1], qyoN[2]), f2(qyoN[2], qyoN[3]), true, ph, any);
   // south faces: (cell k row j, cell k row j+1)
-  const float2 s01 = flux2(f2(z[0], z[1]), f2(h[0], h[1]), f2(zN[0], zN[1]), f2(hN[0], hN[1]),
+  const float2 s01 = flux2<ND>(f2(z[0], z[1]), f2(h[0], h[1]), f2(zN[0], zN[1]), f2(hN[0], hN[1]),
                            f2(qyoN[0], qyoN[1]), f2(qxo[0], qxo[1]), f2(qxo[1], qxo[2]),
                            f2(qxoN[0], qxoN[1]), f2(qxoN[1], qxoN[2]), south, ph, any);
-  const float2 s23 = flux2(f2(z[2], z[3]), f2(h[2], h[3]), f2(zN[2], zN[3]), f2(hN[2], hN[3]),
+  const float2 s23 = flux2<ND>(f2(z[2], z[3]), f2(h[2], h[3]), f2(zN[2], zN[3]), f2(hN[2], hN[3]),
                            f2(qyoN[2], qyoN[3]), f2(qxo[2], qxo[3]), f2(qxo[3], qxoR),
                            f2(qxoN[2], qxoN[3]), f2(qxoN[3], qxoNR), south, ph, any);
   (void)any;
@@ -464,6 +472,7 @@ struct BoolC {
 // would round it the same way in every cell of a binade (a bias in the
 // volume), while the flux term differs from cell to cell.  The reference's
 // clamp between rain and update has no effect there (rain >= 0, depth >= 0).
+template <bool ND>  // FP64 keeps every test of the reference
 __device__ inline void update_cells(double (&hn)[2], const double (&qw)[2], const double (&qe)[2],
                                     const double (&qn)[2], const double (&qs)[2],
                                     const double (&z)[2], bool rain_on, double rain_depth,
@@ -480,13 +489,14 @@ __device__ inline void update_cells(double (&hn)[2], const double (&qw)[2], cons
     hn[k] = v;
   }
 }
+template <bool ND>
 __device__ inline void update_cells(float (&hn)[4], const float (&qw)[4], const float (&qe)[4],
                                     const float (&qn)[4], const float (&qs)[4],
                                     const float (&z)[4], bool rain_on, float rain_depth,
                                     float /*dt*/, float /*dA*/, float dt_dA, float nodata) {
   float rk[4];
 #pragma unroll
-  for (int k = 0; k < 4; k++) rk[k] = (rain_on && z[k] != nodata) ? rain_depth : 0.0f;
+  for (int k = 0; k < 4; k++) rk[k] = (rain_on && (!ND || z[k] != nodata)) ? rain_depth : 0.0f;
 #pragma unroll
   for (int k = 0; k < 4; k += 2) {
     const float2 a = __ffma2_rn(f2(qe[k], qe[k + 1]), f2(-1.0f, -1.0f), f2(qw[k], qw[k + 1]));
@@ -552,6 +562,20 @@ __device__ inline void step_scalars(const StepParams& p, double t, double hmax_p
 // cells (state precision; exact; -FLT_MAX while it has seen none: depths of
 // valid cells are finite and far above it) and, at mass-report steps, its
 // volume and flooded-area sums.
+// A warp's position in its stage ring: the stage it consumes next and the
+// mbarrier phase that stage completes with.  Kept as running counters (the
+// ring depth is 3, so deriving them from a stage count would divide by 3).
+// Packed in one register: bits 0-1 the slot, bit 2 the phase.
+struct RingPos {
+  uint32_t v;
+  __device__ __forceinline__ int slot() const { return (int)(v & 3u); }
+  __device__ __forceinline__ uint32_t phase() const { return v >> 2; }
+  __device__ __forceinline__ void advance() {
+    v = ((v & 3u) == (uint32_t)(kStages - 1)) ? ((v & 4u) ^ 4u) : v + 1u;
+  }
+};
+static_assert(kStages <= 4, "the ring position packs the slot in two bits");
+
 template <typename T>
 struct LaneAcc {
   T m_cell;
@@ -561,14 +585,14 @@ struct LaneAcc {
 
 // One step of strip (sx, sy) of one grid by one warp: the strip's OWN
 // columns and R rows, streamed through the warp's stage ring (`ring`, `bar`;
-// `kglob` = stages the warp has consumed so far, its position in the ring).
+// `pos` = the warp's position in the ring, advanced past the strip's stages).
 // Warps whose strip lies wholly inside the grid in x take a path without the
 // per-column edge tests.  Returns false after a wait time-out, with the
 // copies in flight drained and the grid's status flagged.
 template <typename T>
 __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>& sc, int sx,
                                           int sy, unsigned char (*ring)[4][kRowBytes],
-                                          uint64_t* bar, int& kglob, LaneAcc<T>& acc) {
+                                          uint64_t* bar, RingPos& pos, LaneAcc<T>& acc) {
   constexpr int N = Lanes<T>::N;
   constexpr int OWN = 30 * N;
   static_assert(32 * N * sizeof(T) == kRowBytes, "one 16-byte vector per lane");
@@ -612,9 +636,8 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
   // stage k; lane 0 also posts the expected byte count.  The prologue row
   // j0-1 has no Qy; row ny has only Qy.
   const T* const my_src = lane == 0 ? H : lane == 1 ? Z : lane == 2 ? Qx : Qy;
-  auto issue = [&](int k) {
+  auto issue = [&](int k, int slot) {
     const int r = rfirst + k;
-    const int slot = (kglob + k) % kStages;
     const int a_lo = r < ny ? 0 : 3;
     const int a_hi = r < j0 ? 3 : 4;
     if (lane == 0) mbar_expect_tx(&bar[slot], (uint32_t)((a_hi - a_lo) * kRowBytes));
@@ -623,19 +646,25 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
       bulk_g2s(&ring[slot][lane][0], my_src + (long long)r * P + wcol, kRowBytes, &bar[slot]);
     }
   };
-  for (int k = 0; k < kStages && k < nload; k++) issue(k);
+  {
+    RingPos f = pos;
+    for (int k = 0; k < kStages && k < nload; k++) {
+      issue(k, f.slot());
+      f.advance();
+    }
+  }
   __syncwarp();
-  int kc = 0;  // next stage of this strip to consume
+  int kc = 0;  // next stage of this strip to consume, at ring position `pos`
   auto acquire = [&]() -> const unsigned char* {
-    const int q = kglob + kc;
-    if (!mbar_wait_warp(&bar[q % kStages], (uint32_t)((q / kStages) & 1), kRingWaitLimit))
-      return nullptr;
-    return &ring[q % kStages][0][0] + lane * 16;
+    if (!mbar_wait_warp(&bar[pos.slot()], pos.phase(), kRingWaitLimit)) return nullptr;
+    return &ring[pos.slot()][0][0] + lane * 16;
   };
+  // The consumed stage is refilled with the row kStages ahead (same slot).
   auto release = [&]() {
     __syncwarp();
-    if (kc + kStages < nload) issue(kc + kStages);
+    if (kc + kStages < nload) issue(kc + kStages, pos.slot());
     kc++;
+    pos.advance();
   };
 
   T h[N], z[N], qxo[N], qyo[N], qyn[N];
@@ -693,13 +722,14 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
       const T qxpR = __shfl_down_sync(0xffffffffu, qxp[0], 1);
       const T qxoR = __shfl_down_sync(0xffffffffu, qxo[0], 1);
       T qw_unused[N];
-      row_faces(hp, zp, h, z, qxp, qxo, qyo, qyo, T(0), T(0), T(0), T(0), qxpR, qxoR, true, ph,
-                qw_unused, qyn);
+      row_faces<true>(hp, zp, h, z, qxp, qxo, qyo, qyo, T(0), T(0), T(0), T(0), qxpR, qxoR, true,
+                      ph, qw_unused, qyn);
     }
   }
 
-  auto rows = [&](auto edge_tag) {
+  auto rows = [&](auto edge_tag, auto nd_tag) {
     constexpr bool kEdge = decltype(edge_tag)::value;
+    constexpr bool kND = decltype(nd_tag)::value;
 #pragma unroll kRowUnroll
     for (int j = j0; j < j1; j++) {
       const bool has_next = (j + 1 < ny);
@@ -738,8 +768,8 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
 
       // Faces of the row: interior law everywhere, then the edges.
       T qw[N], qs[N];
-      row_faces(h, z, hN, zN, qxo, qxoN, qyo, qyoN, hL, zL, qyoL, qyoNL, qxoR, qxoNR, has_next,
-                ph, qw, qs);
+      row_faces<kND>(h, z, hN, zN, qxo, qxoN, qyo, qyoN, hL, zL, qyoL, qyoNL, qxoR, qxoNR,
+                     has_next, ph, qw, qs);
       if (kEdge) {
 #pragma unroll
         for (int k = 0; k < N; k++) {
@@ -794,7 +824,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
         sp++;
         next_row = sp < sp_end ? p.spec[sp].row : INT_MAX;
       }
-      update_cells(hn, qw, qe, qyn, qs, z, rain_on, rain_depth, dtT, dAT, dt_dA, ph.nodata);
+      update_cells<kND>(hn, qw, qe, qyn, qs, z, rain_on, rain_depth, dtT, dAT, dt_dA, ph.nodata);
       // Point depth BCs (src/kernels.cpp:259-277), after the update.
       for (int q = sp_row; q < sp; q++) {
         const SpecCell e = p.spec[q];
@@ -829,7 +859,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
         // Hmax over valid cells (a NaN never wins the comparison).
 #pragma unroll
         for (int k = 0; k < N; k++)
-          if ((!kEdge || cb + k < nx) && z[k] != ph.nodata)
+          if ((!kEdge || cb + k < nx) && (!kND || z[k] != ph.nodata))
             acc.m_cell = (hn[k] > acc.m_cell) ? hn[k] : acc.m_cell;
         if (__builtin_expect(mass, 0)) {  // warp-uniform: mass-report steps only
 #pragma unroll
@@ -854,23 +884,37 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
     }
   };
   if (!failed) {
+    // FP32 takes a copy of the row loop without nodata tests on grids that
+    // have no nodata cell; FP64 keeps the reference's tests everywhere.
+    bool nd = true;
+    if constexpr (sizeof(T) == 4) nd = p.has_nodata != 0;
 #if AF_EDGE_SPLIT
     const bool interior = (x0 > 0) && (x0 + OWN < nx);
-    if (interior) rows(BoolC<false>());
-    else rows(BoolC<true>());
 #else
-    rows(BoolC<true>());
+    const bool interior = false;
 #endif
+    if (nd) {
+      if (interior) rows(BoolC<false>(), BoolC<true>());
+      else rows(BoolC<true>(), BoolC<true>());
+    } else {
+      if constexpr (sizeof(T) == 4) {
+        if (interior) rows(BoolC<false>(), BoolC<false>());
+        else rows(BoolC<true>(), BoolC<false>());
+      }
+    }
   }
   if (failed) {
     // Drain the copies still in flight into this warp's stages (bounded),
     // then flag the control block so the loop stops with an error.
     const int issued = min(nload, kc + kStages);
-    for (int k = kc; k < issued; k++)
-      mbar_wait_warp(&bar[(kglob + k) % kStages], (uint32_t)(((kglob + k) / kStages) & 1));
+    RingPos d = pos;
+    for (int k = kc; k < issued; k++) {
+      mbar_wait_warp(&bar[d.slot()], d.phase());
+      d.advance();
+    }
+    for (int k = kc; k < nload; k++) pos.advance();  // past the strip's stages
     if (lane == 0) atomicExch(&p.ctl->status, 2);
   }
-  kglob += nload;
   return !failed;
 }
 
@@ -935,7 +979,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
     fence_mbar_init();
   }
   __syncwarp();
-  int kglob = 0;
+  RingPos pos{0u};
   LaneAcc<T> acc{T(-FLT_MAX), 0.0, 0.0};
   const int tiles_y = (p.nsy + WY - 1) / WY;
   const int ntiles = p.nsx * tiles_y;
@@ -943,7 +987,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
     const int sx = tile % p.nsx;
     const int sy = (tile / p.nsx) * WY + warp;
     if (sy >= p.nsy) continue;
-    if (!run_strip<T>(p, sc, sx, sy, s_ring[warp], bar, kglob, acc)) break;
+    if (!run_strip<T>(p, sc, sx, sy, s_ring[warp], bar, pos, acc)) break;
   }
 
   // A valid cell's depth is finite (NaN never wins a comparison), and in
@@ -1285,7 +1329,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams 
     fence_mbar_init();
   }
   __syncwarp();
-  int kglob = 0;
+  RingPos pos{0u};
   uint32_t rphase = 0;  // completed record fetches, mod 2
   const int units = tab->units;
   const int nact = tab->nact;
@@ -1336,7 +1380,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams 
     const StepScal<T>& sc = *reinterpret_cast<const StepScal<T>*>(rec.scal);
     const int k = u - tab->u0[a];
     LaneAcc<T> acc{T(-FLT_MAX), 0.0, 0.0};
-    ok = run_strip<T>(p, sc, k % p.nsx, k / p.nsx, s_ring[warp], bar, kglob, acc);
+    ok = run_strip<T>(p, sc, k % p.nsx, k / p.nsx, s_ring[warp], bar, pos, acc);
     double m = acc.any_cell() ? (double)acc.m_cell : -DBL_MAX;
     m = warp_maxd(m);
     double v = 0.0, ar = 0.0;

@@ -46,6 +46,9 @@ def test_diverged_state_stops_with_estate(cuda, precision, bad):
         case.h0 = np.zeros((case.ny, case.nx))
         case.h0[case.ny // 2, case.nx // 3] = np.inf
     else:
+        # a wet start, so the first dt already comes from the CFL number (a dry
+        # start takes InitTstep, src/kernels.cpp:36-43)
+        case.h0 = np.full((case.ny, case.nx), 0.5)
         case.cfl = float("nan")
     f = fc.pack(case)
     with Simulation(case, precision, forcing=f) as s:
