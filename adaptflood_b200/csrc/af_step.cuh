@@ -37,6 +37,17 @@
 #include "af_common.cuh"
 #include "af_pow.cuh"
 
+// FP32 face-law shape: 1 selects the upstream side once per face and forms
+// |Qv| hflow^(-7/3) as one exp2 (see flux2).
+#ifndef AF_FLUX_V2
+#define AF_FLUX_V2 0
+#endif
+// 1: FP32 grids without nodata cells take a copy of the row loop without the
+// nodata tests.
+#ifndef AF_NODATA_SPLIT
+#define AF_NODATA_SPLIT 1
+#endif
+
 namespace af {
 
 // Device control block of one simulation.
@@ -312,8 +323,17 @@ __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float
   // quantities from differences of close values (exact or nearly so).
   const float2 dz = __fadd2_rn(z0, f2(-z1.x, -z1.y));
   const float2 dh = __fadd2_rn(dz, __fadd2_rn(h0, f2(-h1.x, -h1.y)));
+#if AF_FLUX_V2
+  // the upstream cell's depth and its bed's drop to the other cell, selected
+  // once, then one packed add (the same values as forming both sides)
+  const bool ux = dh.x >= 0.0f, uy = dh.y >= 0.0f;
+  const float2 hup = f2(ux ? h0.x : h1.x, uy ? h0.y : h1.y);
+  const float2 drop = f2(fminf(0.0f, ux ? dz.x : -dz.x), fminf(0.0f, uy ? dz.y : -dz.y));
+  const float2 hfx = __fadd2_rn(hup, drop);
+#else
   const float2 hfx = f2(dh.x >= 0.0f ? h0.x + fminf(0.0f, dz.x) : h1.x + fminf(0.0f, -dz.x),
                         dh.y >= 0.0f ? h0.y + fminf(0.0f, dz.y) : h1.y + fminf(0.0f, -dz.y));
+#endif
   // The reference clamps the flow depth to [0, MaxHflow] and calls the face
   // wet above DepthThresh; with DepthThresh >= 0 (fill_scalars makes the FP32
   // threshold so) the clamp at 0 only matters for faces that are dry either
@@ -333,9 +353,19 @@ __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float
   const float2 qavg = __fmul2_rn(__fadd2_rn(__fadd2_rn(qa, qb), __fadd2_rn(qc, qd)),
                                  f2(0.25f, 0.25f));
   const float2 qv2 = __ffma2_rn(q0, q0, __fmul2_rn(qavg, qavg));
+#if AF_FLUX_V2
+  // |Qv| * hflow^(-7/3) = 2^(log2(Qv^2)/2 - 7/3 log2(hflow)) on the SFU (Qv = 0
+  // gives 2^-inf = 0, a friction-free face, as in the reference)
+  const float2 lg = __ffma2_rn(f2(__log2f(qv2.x), __log2f(qv2.y)), f2(0.5f, 0.5f),
+                               __fmul2_rn(f2(__log2f(hf.x), __log2f(hf.y)),
+                                          f2(-7.0f / 3.0f, -7.0f / 3.0f)));
+  const float2 den = __ffma2_rn(f2(ph.gdt_fn2, ph.gdt_fn2), f2(exp2f(lg.x), exp2f(lg.y)),
+                                f2(1.0f, 1.0f));
+#else
   const float2 qv = f2(sqrtf(qv2.x), sqrtf(qv2.y));
   const float2 pw = f2(exp2f(-7.0f / 3.0f * __log2f(hf.x)), exp2f(-7.0f / 3.0f * __log2f(hf.y)));
   const float2 den = __ffma2_rn(__fmul2_rn(f2(ph.gdt_fn2, ph.gdt_fn2), qv), pw, f2(1.0f, 1.0f));
+#endif
   return f2(wx ? __fdividef(num.x, den.x) : 0.0f, wy ? __fdividef(num.y, den.y) : 0.0f);
 }
 
@@ -378,6 +408,7 @@ __device__ inline void row_faces(const float (&h)[4], const float (&z)[4], const
 #ifndef AF_STAGES
 #define AF_STAGES 3
 #endif
+
 constexpr int kStages = AF_STAGES;  // ring depth (rows in flight per warp, incl. the one in use)
 // Code-shape knobs of the fused step (compile time): unroll factor of the row
 // loop, and whether x-interior strips get their own copy of the row body
@@ -887,7 +918,9 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
     // FP32 takes a copy of the row loop without nodata tests on grids that
     // have no nodata cell; FP64 keeps the reference's tests everywhere.
     bool nd = true;
+#if AF_NODATA_SPLIT
     if constexpr (sizeof(T) == 4) nd = p.has_nodata != 0;
+#endif
 #if AF_EDGE_SPLIT
     const bool interior = (x0 > 0) && (x0 + OWN < nx);
 #else

@@ -181,10 +181,12 @@ def write_dem(path: str, dem: np.ndarray, xll: float, yll: float, cs: float,
 
 
 # ---------------------------------------------------------------- terrain
-def _value_noise_rows(lat: np.ndarray, spacing: float, j0: int, j1: int, nx: int) -> np.ndarray:
-    """Smooth value noise in [-1, 1] for rows j0..j1 from a random lattice."""
+def _value_noise_rows(lat: np.ndarray, spacing: float, j0: int, j1: int, nx: int,
+                      x0: int = 0) -> np.ndarray:
+    """Smooth value noise in [-1, 1] for rows j0..j1, columns x0..x0+nx, from a
+    random lattice."""
     y = (np.arange(j0, j1, dtype=np.float64) + 0.5) / spacing
-    x = (np.arange(nx, dtype=np.float64) + 0.5) / spacing
+    x = (np.arange(x0, x0 + nx, dtype=np.float64) + 0.5) / spacing
     iy = np.floor(y).astype(np.int64)
     ix = np.floor(x).astype(np.int64)
     fy = y - iy
@@ -202,11 +204,19 @@ def _value_noise_rows(lat: np.ndarray, spacing: float, j0: int, j1: int, nx: int
 
 def make_dem(nx: int, ny: int, dx: float, seed: int, slope: float = 0.001,
              amplitude: float = 0.5, channel_depth: float = 3.0, channel_width: int = 5,
-             ponds: int = 0, pond_depth=(0.5, 2.0), rows_per_chunk: int = 512) -> np.ndarray:
+             ponds: int = 0, pond_depth=(0.5, 2.0), rows_per_chunk: int = 512,
+             window=None) -> np.ndarray:
     """Plane sloping ``slope`` toward the south + 2-octave seeded noise of
     amplitude ``amplitude`` (a product of sinusoids plus two octaves of value
     noise) + an N-S channel ``channel_width`` cells wide, ``channel_depth``
-    deep, centred on column nx//2; optional Gaussian ponds."""
+    deep, centred on column nx//2; optional Gaussian ponds.
+
+    ``window`` = (x0, y0, w, h) returns only that window of the nx x ny DEM,
+    computed cell by cell with the same expressions (the same values as a
+    crop of the whole DEM, without building it)."""
+    x0, y0, wx, wy = window if window is not None else (0, 0, nx, ny)
+    if not (0 <= x0 and 0 <= y0 and x0 + wx <= nx and y0 + wy <= ny):
+        raise ValueError("window outside the grid")
     rng = np.random.default_rng(seed)
     s1 = max(4.0, min(nx, ny) / 8.0)
     s2 = s1 / 2.0
@@ -215,33 +225,37 @@ def make_dem(nx: int, ny: int, dx: float, seed: int, slope: float = 0.001,
     lx = rng.uniform(0.15, 0.35) * nx
     ly = rng.uniform(0.15, 0.35) * ny
     px, py = rng.uniform(0, 2 * math.pi, size=2)
-    dem = np.empty((ny, nx), dtype=np.float64)
-    xs = np.arange(nx, dtype=np.float64)
+    dem = np.empty((wy, wx), dtype=np.float64)
+    xs = np.arange(x0, x0 + wx, dtype=np.float64)
     sinx = np.sin(2 * math.pi * xs / lx + px)
     c0 = max(0, nx // 2 - channel_width // 2)
     c1 = min(nx, c0 + channel_width)
-    for j0 in range(0, ny, rows_per_chunk):
-        j1 = min(ny, j0 + rows_per_chunk)
+    c0w, c1w = max(c0, x0) - x0, min(c1, x0 + wx) - x0  # the channel inside the window
+    for j0 in range(y0, y0 + wy, rows_per_chunk):
+        j1 = min(y0 + wy, j0 + rows_per_chunk)
         ys = np.arange(j0, j1, dtype=np.float64)
         siny = np.sin(2 * math.pi * ys / ly + py)
         n = 0.5 * (siny[:, None] * sinx[None, :])
-        n += 0.3 * _value_noise_rows(lat1, s1, j0, j1, nx)
-        n += 0.2 * _value_noise_rows(lat2, s2, j0, j1, nx)
+        n += 0.3 * _value_noise_rows(lat1, s1, j0, j1, wx, x0)
+        n += 0.2 * _value_noise_rows(lat2, s2, j0, j1, wx, x0)
         z = slope * (ny - 1 - ys)[:, None] * dx + amplitude * n
-        if channel_depth and c1 > c0:
-            z[:, c0:c1] -= channel_depth
-        dem[j0:j1] = z
+        if channel_depth and c1w > c0w:
+            z[:, c0w:c1w] -= channel_depth
+        dem[j0 - y0:j1 - y0] = z
     for _ in range(ponds):
         ci, cj = rng.uniform(0, nx), rng.uniform(0, ny)
         r = rng.uniform(0.004, 0.02) * min(nx, ny) + 2.0
         depth = rng.uniform(*pond_depth)
         i0, i1 = int(max(0, ci - 3 * r)), int(min(nx, ci + 3 * r + 1))
         j0, j1 = int(max(0, cj - 3 * r)), int(min(ny, cj + 3 * r + 1))
+        i0, i1 = max(i0, x0), min(i1, x0 + wx)
+        j0, j1 = max(j0, y0), min(j1, y0 + wy)
         if i1 <= i0 or j1 <= j0:
             continue
         gi = np.arange(i0, i1) + 0.5 - ci
         gj = np.arange(j0, j1) + 0.5 - cj
-        dem[j0:j1, i0:i1] -= depth * np.exp(-(gj[:, None] ** 2 + gi[None, :] ** 2) / (2 * r * r))
+        dem[j0 - y0:j1 - y0, i0 - x0:i1 - x0] -= depth * np.exp(
+            -(gj[:, None] ** 2 + gi[None, :] ** 2) / (2 * r * r))
     return dem
 
 
@@ -328,14 +342,36 @@ def config2(seed: int = 2, n: int = 8192, dx: float = 5.0, sources: int = 4096) 
     return c
 
 
-def config3(seed: int = 3, n: int = 16384, dx: float = 2.0, block: int = 512) -> Case:
-    """16384x16384 at 2 m with Gaussian ponds and a 1 m deep reservoir block."""
-    dem = make_dem(n, n, dx, seed, ponds=max(8, (n // 256) ** 2 // 4))
+def config3(seed: int = 3, n: int = 16384, dx: float = 2.0, block: int = 512,
+            channel: bool = True) -> Case:
+    """16384x16384 at 2 m with Gaussian ponds and a 1 m deep reservoir block.
+    At full size the reservoir (at n/4) is 8 km from the DEM's 3 m deep
+    channel (at n/2), which its water does not reach in the 3 h simulated;
+    reduced grids that keep the reservoir should drop the channel
+    (channel=False): deep water in it in a closed box is outside the stable
+    regime of the scheme."""
+    dem = make_dem(n, n, dx, seed, ponds=max(8, (n // 256) ** 2 // 4),
+                   channel_depth=3.0 if channel else 0.0)
     h0 = np.zeros((n, n), dtype=np.float64)
     b0 = n // 4
     h0[b0:b0 + block, b0:b0 + block] = 1.0
     return Case(n, n, dx, dem, h0=h0, sim_time=10800.0, save_int=3600.0, mass_int=600.0,
                 cfl=0.7, fpn=0.035, depth_thresh=0.001, name=f"c3_{n}")
+
+
+def config3_window(w: int = 1024, seed: int = 3, n: int = 16384, dx: float = 2.0,
+                   block: int = 512) -> Case:
+    """A w x w window of the C3 configuration centred on its reservoir: the
+    same terrain, ponds and 1 m deep reservoir block cell for cell (closed
+    edges at the window), without building the full grid."""
+    b0 = n // 4
+    x0 = y0 = max(0, b0 + block // 2 - w // 2)
+    dem = make_dem(n, n, dx, seed, ponds=max(8, (n // 256) ** 2 // 4), window=(x0, y0, w, w))
+    h0 = np.zeros((w, w), dtype=np.float64)
+    r0 = b0 - y0
+    h0[max(0, r0):r0 + block, max(0, r0):r0 + block] = 1.0
+    return Case(w, w, dx, dem, h0=h0, sim_time=10800.0, save_int=3600.0, mass_int=600.0,
+                cfl=0.7, fpn=0.035, depth_thresh=0.001, name=f"c3_window_{w}")
 
 
 def ensemble_case(rng: np.random.Generator, seed: int, lo: int = 256, hi: int = 2048,

@@ -9,7 +9,10 @@ the host build.
 Bars: on depths (1 mm .. 10 m, the flux law's range) and on a wide range, at
 most 1e-6 of arguments may differ from the C library (measured about 1.3e-7,
 each a single ulp); special values agree exactly; the device build equals the
-host build bit for bit.
+host build bit for bit wherever the table path runs (|y log x| < 512: for
+y = 10/3 every x between 1e-66 and 1e66).  Beyond that each build falls back
+to its platform's pow (CUDA's on the device), which can differ from the C
+library's in the last bit; no depth comes near that range.
 """
 import ctypes as C
 import os
@@ -90,7 +93,7 @@ def test_tables_are_what_the_generator_writes():
 def test_device_pow_equals_host_restatement(cuda):
     import torch
     from adaptflood_b200 import _lib
-    x = np.concatenate([_samples(21, 1 << 22, 1e-3, 10.0), _samples(22, 1 << 18, 1e-200, 1e200),
+    x = np.concatenate([_samples(21, 1 << 22, 1e-3, 10.0), _samples(22, 1 << 18, 1e-60, 1e60),
                         SPECIAL])
     want = _restated(x)
     gx = torch.from_numpy(x).cuda()
