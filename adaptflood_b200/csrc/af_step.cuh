@@ -42,6 +42,10 @@
 #ifndef AF_FLUX_V2
 #define AF_FLUX_V2 0
 #endif
+// 1: one lane issues each row's bulk copies (else four lanes, one array each).
+#ifndef AF_ISSUE_ONE_LANE
+#define AF_ISSUE_ONE_LANE 0
+#endif
 // 1: FP32 grids without nodata cells take a copy of the row loop without the
 // nodata tests.
 #ifndef AF_NODATA_SPLIT
@@ -666,6 +670,27 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
   // Lanes 0..3 each copy one array (H, DEM, Qx, Qy) of row rfirst+k into
   // stage k; lane 0 also posts the expected byte count.  The prologue row
   // j0-1 has no Qy; row ny has only Qy.
+#if AF_ISSUE_ONE_LANE
+  // Lane 0 issues the row's copies (straight-line code, no per-lane
+  // serialisation of the copy instruction); the warp's reads of the stage
+  // being refilled are ordered before them by the __syncwarp in release().
+  auto issue = [&](int k, int slot) {
+    const int r = rfirst + k;
+    if (lane == 0) {
+      const int a_lo = r < ny ? 0 : 3;
+      const int a_hi = r < j0 ? 3 : 4;
+      const long long off = (long long)r * P + wcol;
+      mbar_expect_tx(&bar[slot], (uint32_t)((a_hi - a_lo) * kRowBytes));
+      fence_proxy_async();
+      if (a_lo == 0) {
+        bulk_g2s(&ring[slot][0][0], H + off, kRowBytes, &bar[slot]);
+        bulk_g2s(&ring[slot][1][0], Z + off, kRowBytes, &bar[slot]);
+        bulk_g2s(&ring[slot][2][0], Qx + off, kRowBytes, &bar[slot]);
+      }
+      if (a_hi == 4) bulk_g2s(&ring[slot][3][0], Qy + off, kRowBytes, &bar[slot]);
+    }
+  };
+#else
   const T* const my_src = lane == 0 ? H : lane == 1 ? Z : lane == 2 ? Qx : Qy;
   auto issue = [&](int k, int slot) {
     const int r = rfirst + k;
@@ -677,6 +702,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
       bulk_g2s(&ring[slot][lane][0], my_src + (long long)r * P + wcol, kRowBytes, &bar[slot]);
     }
   };
+#endif
   {
     RingPos f = pos;
     for (int k = 0; k < kStages && k < nload; k++) {
