@@ -46,11 +46,6 @@
 #ifndef AF_ISSUE_ONE_LANE
 #define AF_ISSUE_ONE_LANE 0
 #endif
-// 1: FP32 grids without nodata cells take a copy of the row loop without the
-// nodata tests.
-#ifndef AF_NODATA_SPLIT
-#define AF_NODATA_SPLIT 1
-#endif
 
 namespace af {
 
@@ -624,7 +619,10 @@ struct LaneAcc {
 // Warps whose strip lies wholly inside the grid in x take a path without the
 // per-column edge tests.  Returns false after a wait time-out, with the
 // copies in flight drained and the grid's status flagged.
-template <typename T>
+// kSplitND: FP32 grids without nodata cells take a copy of the row loop
+// without the nodata tests (the same results; the batch kernel uses it, the
+// single-grid kernel measured no faster with it).
+template <typename T, bool kSplitND = false>
 __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>& sc, int sx,
                                           int sy, unsigned char (*ring)[4][kRowBytes],
                                           uint64_t* bar, RingPos& pos, LaneAcc<T>& acc) {
@@ -944,9 +942,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
     // FP32 takes a copy of the row loop without nodata tests on grids that
     // have no nodata cell; FP64 keeps the reference's tests everywhere.
     bool nd = true;
-#if AF_NODATA_SPLIT
-    if constexpr (sizeof(T) == 4) nd = p.has_nodata != 0;
-#endif
+    if constexpr (sizeof(T) == 4 && kSplitND) nd = p.has_nodata != 0;
 #if AF_EDGE_SPLIT
     const bool interior = (x0 > 0) && (x0 + OWN < nx);
 #else
@@ -956,7 +952,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
       if (interior) rows(BoolC<false>(), BoolC<true>());
       else rows(BoolC<true>(), BoolC<true>());
     } else {
-      if constexpr (sizeof(T) == 4) {
+      if constexpr (sizeof(T) == 4 && kSplitND) {
         if (interior) rows(BoolC<false>(), BoolC<false>());
         else rows(BoolC<true>(), BoolC<false>());
       }
@@ -1439,7 +1435,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams 
     const StepScal<T>& sc = *reinterpret_cast<const StepScal<T>*>(rec.scal);
     const int k = u - tab->u0[a];
     LaneAcc<T> acc{T(-FLT_MAX), 0.0, 0.0};
-    ok = run_strip<T>(p, sc, k % p.nsx, k / p.nsx, s_ring[warp], bar, pos, acc);
+    ok = run_strip<T, true>(p, sc, k % p.nsx, k / p.nsx, s_ring[warp], bar, pos, acc);
     double m = acc.any_cell() ? (double)acc.m_cell : -DBL_MAX;
     m = warp_maxd(m);
     double v = 0.0, ar = 0.0;
