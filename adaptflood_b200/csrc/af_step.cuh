@@ -37,6 +37,11 @@
 #include "af_common.cuh"
 #include "af_pow.cuh"
 
+// Batch kernel: 1 hands out units past the first round from a per-step
+// counter (dynamic), 0 assigns unit w + k*W to warp w (static).
+#ifndef AF_BATCH_DYNAMIC
+#define AF_BATCH_DYNAMIC 0
+#endif
 // FP32 face-law shape: 1 selects the upstream side once per face and forms
 // |Qv| hflow^(-7/3) as one exp2 (see flux2).
 #ifndef AF_FLUX_V2
@@ -1177,6 +1182,8 @@ struct BatchCtl {
   int stop_on_done;
   int done;             // or when nothing is active or the host asks for attention
   int status;           // nonzero: a wait timed out; the batch's state is invalid
+  unsigned int next_unit;  // units of the coming step handed out past the first round
+  int pad_;
   // Optional per-step trace (af_batch_set_trace): record k describes batch
   // step trace_base + k as {start, end} on the device clock (ns) and the
   // cells and strips it stepped.  Written by the host between launches.
@@ -1274,6 +1281,7 @@ __global__ void __launch_bounds__(kFoldThreads) k_batch_begin(const BatchParams 
     b->step_stop = (max_steps > (long long)0x3FFFFFFFFFFFFFFFLL - s) ? 0x3FFFFFFFFFFFFFFFLL
                                                                      : s + max_steps;
     b->completed = 0;
+    b->next_unit = 0u;
     b->stop_on_done = stop_on_done;
     const int done = nact == 0 || max_steps <= 0 || b->status != 0;
     b->done = done;
@@ -1344,6 +1352,7 @@ __global__ void __launch_bounds__(kFoldThreads) k_batch_fold(const BatchParams b
   }
   if (threadIdx.x == 0) {
     const long long step_new = b->step + 1;
+    b->next_unit = 0u;  // the next step hands out its units afresh
     b->step = step_new;
     b->completed += ndone;
     const bool attn = bp.attention != nullptr && *bp.attention != 0;
@@ -1424,7 +1433,18 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams 
   if (!ok) mbar_wait_warp(rbar, rphase ^ 1u);  // drain the copy before leaving
   while (ok) {
     // The next unit's scenario; its record is fetched while this unit runs.
+#if AF_BATCH_DYNAMIC
+    // After the first round a warp takes the next unfinished unit from the
+    // step's counter (fetched one unit ahead, so the record prefetch still
+    // overlaps): warps that finish early take more, none idles while units
+    // remain.  Units keep their order, so warps running at once still read
+    // neighbouring strips of the same rows.
+    int un = 0;
+    if (lane == 0) un = W + (int)atomicAdd(&bp.bctl->next_unit, 1u);
+    un = __shfl_sync(0xffffffffu, un, 0);
+#else
     const int un = u + W;
+#endif
     const int an = un < units ? scen_of(a, un) : a;
     const int slot_n = un < units ? tab->act[an] : -1;
     const bool refetch = slot_n >= 0 && slot_n != slot;
