@@ -37,6 +37,15 @@
 #include "af_common.cuh"
 #include "af_pow.cuh"
 
+// FP32 face-law experiments: AF_FRICTION 1 evaluates the friction factors
+// correctly rounded; AF_FACE_FORM 1 forms the flow depth from surface
+// elevations.  Both 0 in the library.
+#ifndef AF_FRICTION
+#define AF_FRICTION 0
+#endif
+#ifndef AF_FACE_FORM
+#define AF_FACE_FORM 0
+#endif
 // Batch kernel: 1 hands out units past the first round from a per-step
 // counter (dynamic), 0 assigns unit w + k*W to warp w (static).
 #ifndef AF_BATCH_DYNAMIC
@@ -326,8 +335,16 @@ __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float
   // max(y0,y1) - max(z0,z1) = h_up + min(0, z_up - z_down) are the same
   // quantities from differences of close values (exact or nearly so).
   const float2 dz = __fadd2_rn(z0, f2(-z1.x, -z1.y));
+#if AF_FACE_FORM == 1
+  const float2 dh = __fadd2_rn(__fadd2_rn(z0, h0), f2(-(z1.x + h1.x), -(z1.y + h1.y)));
+#else
   const float2 dh = __fadd2_rn(dz, __fadd2_rn(h0, f2(-h1.x, -h1.y)));
-#if AF_FLUX_V2
+#endif
+#if AF_FACE_FORM == 1
+  // flow depth from surface elevations y = z + h (the reference's form in FP32)
+  const float2 hfx = f2(fmaxf(z0.x + h0.x, z1.x + h1.x) - fmaxf(z0.x, z1.x),
+                        fmaxf(z0.y + h0.y, z1.y + h1.y) - fmaxf(z0.y, z1.y));
+#elif AF_FLUX_V2
   // the upstream cell's depth and its bed's drop to the other cell, selected
   // once, then one packed add (the same values as forming both sides)
   const bool ux = dh.x >= 0.0f, uy = dh.y >= 0.0f;
@@ -357,7 +374,13 @@ __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float
   const float2 qavg = __fmul2_rn(__fadd2_rn(__fadd2_rn(qa, qb), __fadd2_rn(qc, qd)),
                                  f2(0.25f, 0.25f));
   const float2 qv2 = __ffma2_rn(q0, q0, __fmul2_rn(qavg, qavg));
-#if AF_FLUX_V2
+#if AF_FRICTION == 1
+  // correctly rounded friction factors (a diagnostic form: FP64 pow)
+  const float2 qv = f2(__fsqrt_rn(qv2.x), __fsqrt_rn(qv2.y));
+  const float2 pw = f2((float)pow((double)hf.x, -7.0 / 3.0), (float)pow((double)hf.y, -7.0 / 3.0));
+  const float2 den = __ffma2_rn(__fmul2_rn(f2(ph.gdt_fn2, ph.gdt_fn2), qv), pw, f2(1.0f, 1.0f));
+  return f2(wx ? __fdiv_rn(num.x, den.x) : 0.0f, wy ? __fdiv_rn(num.y, den.y) : 0.0f);
+#elif AF_FLUX_V2
   // |Qv| * hflow^(-7/3) = 2^(log2(Qv^2)/2 - 7/3 log2(hflow)) on the SFU (Qv = 0
   // gives 2^-inf = 0, a friction-free face, as in the reference)
   const float2 lg = __ffma2_rn(f2(__log2f(qv2.x), __log2f(qv2.y)), f2(0.5f, 0.5f),
