@@ -130,23 +130,48 @@ def report(case: sc.Case, device: int = 0, input_rounding: bool = False) -> dict
     return out
 
 
+# A scenario is called well-conditioned when FP64 arithmetic on its inputs
+# rounded to FP32 stays this close to plain FP64 (a tenth of the FP32 bars).
+COND_DEPTH_M, COND_MASS = 1e-4, 1e-7
+
+
 def _scenario_errors(cases, results32, device):
     """Per scenario: the FP32 result (depth field, end volume) against the
-    scenario's own FP64 single-grid run."""
+    scenario's own FP64 single-grid run, and the scenario's conditioning: the
+    same errors of FP64 on the FP32-rounded DEM (and start depth)."""
     rows = []
     for case, (H32, vol32) in zip(cases, results32):
         r64 = run(case, "f64", device)
+        rr = run(rounded_inputs(case), "f64", device)
         valid = case.dem != case.nodata
         err = np.abs((H32 - r64["H"])[valid])
-        rows.append({"name": case.name, "cells": case.cells, "dx": case.dx,
-                     "max_depth_error_m": float(err.max()) if err.size else 0.0,
-                     "relative_mass_error_end": abs(vol32 - r64["vol"]) /
-                     max(abs(r64["vol"]), 1e-300)})
-    md = [r["max_depth_error_m"] for r in rows]
-    mm = [r["relative_mass_error_end"] for r in rows]
-    return {"scenarios": len(rows), "max_depth_error_m": max(md),
-            "median_max_depth_error_m": float(np.median(md)),
-            "relative_mass_error_max": max(mm), "relative_mass_error_median": float(np.median(mm)),
+        cerr = np.abs((rr["H"] - r64["H"])[valid])
+        v64 = max(abs(r64["vol"]), 1e-300)
+        row = {"name": case.name, "cells": case.cells, "dx": case.dx,
+               "max_depth_error_m": float(err.max()) if err.size else 0.0,
+               "relative_mass_error_end": abs(vol32 - r64["vol"]) / v64,
+               "conditioning_depth_m": float(cerr.max()) if cerr.size else 0.0,
+               "conditioning_mass": abs(rr["vol"] - r64["vol"]) / v64}
+        row["well_conditioned"] = (row["conditioning_depth_m"] <= COND_DEPTH_M and
+                                   row["conditioning_mass"] <= COND_MASS)
+        rows.append(row)
+
+    def stats(rs):
+        if not rs:
+            return {"scenarios": 0}
+        md = [r["max_depth_error_m"] for r in rs]
+        mm = [r["relative_mass_error_end"] for r in rs]
+        return {"scenarios": len(rs), "max_depth_error_m": max(md),
+                "median_max_depth_error_m": float(np.median(md)),
+                "relative_mass_error_max": max(mm),
+                "relative_mass_error_median": float(np.median(mm)),
+                "within_bars": sum(1 for r in rs if r["max_depth_error_m"] <= 1e-3 and
+                                   r["relative_mass_error_end"] <= 1e-6)}
+    good = [r for r in rows if r["well_conditioned"]]
+    return {**stats(rows), "well_conditioned": stats(good),
+            "ill_conditioned": stats([r for r in rows if not r["well_conditioned"]]),
+            "conditioning_rule": f"FP64 on FP32-rounded inputs within {COND_DEPTH_M} m and "
+                                 f"{COND_MASS} relative mass of plain FP64",
             "per_scenario": rows,
             "tolerance": {"max_depth_error_m": 1e-3, "relative_mass_error": 1e-6}}
 
