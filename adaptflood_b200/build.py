@@ -4,7 +4,12 @@ Floating-point flags per translation unit:
   * af_plain.cu, af_step_f64.cu, af_sim.cu: -fmad=false, so FP64 expressions
     round exactly as the reference's C++ does on the CPU;
   * af_step_f32.cu: -use_fast_math (FP32 path: FMA contraction, approximate
-    division/sqrt and SFU exp2/log2 are within its error budget).
+    division/sqrt and SFU exp2/log2 are within its error budget).  The flag
+    also lets the compiler contract the FP64 bookkeeping compiled in this unit
+    for the FP32 kernels (time t + dt, the CFL dt, hydrograph and rain
+    interpolation, the compensated volume sums) into fused multiply-adds: those
+    FP64 values may differ from the FP64 path's in the last bit, far inside the
+    FP32 path's tolerance, and the same in its single-grid and batch kernels.
 Host code is compiled with -ffp-contract=off for the same reason.
 """
 from __future__ import annotations
