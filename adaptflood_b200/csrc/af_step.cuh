@@ -38,8 +38,9 @@
 #include "af_pow.cuh"
 
 // FP32 face-law experiments: AF_FRICTION 1 evaluates the friction factors
-// correctly rounded; AF_FACE_FORM 1 forms the flow depth from surface
-// elevations.  Both 0 in the library.
+// correctly rounded; AF_FACE_FORM 1 forms the flow depth and the head
+// difference from surface elevations (2: the flow depth only, 3: the head
+// difference only).  Both 0 in the library.
 #ifndef AF_FRICTION
 #define AF_FRICTION 0
 #endif
@@ -49,7 +50,7 @@
 // Batch kernel: 1 hands out units past the first round from a per-step
 // counter (dynamic), 0 assigns unit w + k*W to warp w (static).
 #ifndef AF_BATCH_DYNAMIC
-#define AF_BATCH_DYNAMIC 0
+#define AF_BATCH_DYNAMIC 1
 #endif
 // FP32 face-law shape: 1 selects the upstream side once per face and forms
 // |Qv| hflow^(-7/3) as one exp2 (see flux2).
@@ -335,12 +336,12 @@ __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float
   // max(y0,y1) - max(z0,z1) = h_up + min(0, z_up - z_down) are the same
   // quantities from differences of close values (exact or nearly so).
   const float2 dz = __fadd2_rn(z0, f2(-z1.x, -z1.y));
-#if AF_FACE_FORM == 1
+#if AF_FACE_FORM == 1 || AF_FACE_FORM == 3
   const float2 dh = __fadd2_rn(__fadd2_rn(z0, h0), f2(-(z1.x + h1.x), -(z1.y + h1.y)));
 #else
   const float2 dh = __fadd2_rn(dz, __fadd2_rn(h0, f2(-h1.x, -h1.y)));
 #endif
-#if AF_FACE_FORM == 1
+#if AF_FACE_FORM == 1 || AF_FACE_FORM == 2
   // flow depth from surface elevations y = z + h (the reference's form in FP32)
   const float2 hfx = f2(fmaxf(z0.x + h0.x, z1.x + h1.x) - fmaxf(z0.x, z1.x),
                         fmaxf(z0.y + h0.y, z1.y + h1.y) - fmaxf(z0.y, z1.y));
