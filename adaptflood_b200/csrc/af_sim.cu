@@ -295,11 +295,14 @@ static int pick_shape(Sim& s) {
   // number of strips and each is as short as it can be (measured against
   // powers of two: 512^2 +21 %, 2048^2 +6 %, 4096^2 +5 %).  The FP64 step,
   // bound by its arithmetic, keeps more, shorter strips on mid-size grids
-  // (measured 8-9 % faster than the two-wave rule at 2048^2 and 4096^2).
+  // (measured 8-9 % faster than the two-wave rule at 2048^2 and 4096^2), and
+  // on grids of up to 2^20 cells (less than one wave) two-row strips, the
+  // shortest serial chain per warp (512^2: 34.7 ms for the 1442-step C1 run
+  // against 50.2 ms with four rows).
   const long long cells = (long long)s.c.nx * s.c.ny;
   s.R = 32;
   if (s.prec == AF_PREC_F64) {
-    if (cells <= (1LL << 20)) s.R = 4;
+    if (cells <= (1LL << 20)) s.R = 2;
     else if (cells <= (1LL << 23)) s.R = 8;
     else if (cells <= (1LL << 25)) s.R = 16;
   } else {
