@@ -131,8 +131,7 @@ CHILD = textwrap.dedent("""
 
 
 def test_ring_wait_timeout_reports_estate(cuda):
-    if not os.path.exists(B.WAITTEST_LIB):
-        B.build_wait_test()
+    B.build_wait_test()  # incremental: rebuilds only what changed since the last build
     env = dict(os.environ, AF_LIB_PATH=B.WAITTEST_LIB)
     r = subprocess.run([sys.executable, "-c", CHILD.format(root=ROOT)], env=env,
                        capture_output=True, text=True, timeout=300)
