@@ -694,6 +694,13 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
   // (all four; row ny only exists for Qy).
   const int rfirst = j0 > 0 ? j0 - 1 : j0;
   const int nload = j1 + 1 - rfirst;
+  // Bytes of each row copy: the whole window, or on a grid's last strip in x
+  // the columns up to nx (Qx's east edge face) rounded up to 16 bytes, so the
+  // padding past the grid is not read.  The lanes past it see stale stage
+  // bytes; every result of theirs is masked (stores, Hmax, volume), and the
+  // last valid lane's right-hand neighbour values (Qx at column nx) are copied.
+  const uint32_t row_bytes = (uint32_t)min(
+      (long long)kRowBytes, (((long long)nx + 1 - wcol) * (long long)sizeof(T) + 15) & ~15LL);
   // Lanes 0..3 each copy one array (H, DEM, Qx, Qy) of row rfirst+k into
   // stage k; lane 0 also posts the expected byte count.  The prologue row
   // j0-1 has no Qy; row ny has only Qy.
@@ -707,14 +714,14 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
       const int a_lo = r < ny ? 0 : 3;
       const int a_hi = r < j0 ? 3 : 4;
       const long long off = (long long)r * P + wcol;
-      mbar_expect_tx(&bar[slot], (uint32_t)((a_hi - a_lo) * kRowBytes));
+      mbar_expect_tx(&bar[slot], (uint32_t)(a_hi - a_lo) * row_bytes);
       fence_proxy_async();
       if (a_lo == 0) {
-        bulk_g2s(&ring[slot][0][0], H + off, kRowBytes, &bar[slot]);
-        bulk_g2s(&ring[slot][1][0], Z + off, kRowBytes, &bar[slot]);
-        bulk_g2s(&ring[slot][2][0], Qx + off, kRowBytes, &bar[slot]);
+        bulk_g2s(&ring[slot][0][0], H + off, row_bytes, &bar[slot]);
+        bulk_g2s(&ring[slot][1][0], Z + off, row_bytes, &bar[slot]);
+        bulk_g2s(&ring[slot][2][0], Qx + off, row_bytes, &bar[slot]);
       }
-      if (a_hi == 4) bulk_g2s(&ring[slot][3][0], Qy + off, kRowBytes, &bar[slot]);
+      if (a_hi == 4) bulk_g2s(&ring[slot][3][0], Qy + off, row_bytes, &bar[slot]);
     }
   };
 #else
@@ -723,10 +730,10 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
     const int r = rfirst + k;
     const int a_lo = r < ny ? 0 : 3;
     const int a_hi = r < j0 ? 3 : 4;
-    if (lane == 0) mbar_expect_tx(&bar[slot], (uint32_t)((a_hi - a_lo) * kRowBytes));
+    if (lane == 0) mbar_expect_tx(&bar[slot], (uint32_t)(a_hi - a_lo) * row_bytes);
     if (lane >= a_lo && lane < a_hi) {
       fence_proxy_async();
-      bulk_g2s(&ring[slot][lane][0], my_src + (long long)r * P + wcol, kRowBytes, &bar[slot]);
+      bulk_g2s(&ring[slot][lane][0], my_src + (long long)r * P + wcol, row_bytes, &bar[slot]);
     }
   };
 #endif
