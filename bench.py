@@ -11,7 +11,7 @@ and the Hmax reduction that sets the next dt.
 Our arm times K steps of the fused kernel (one CUDA-graph launch, CUDA events
 on the simulation's stream) in FP32 (the headline `value`) and FP64, reports
 the HBM roofline of the step kernel, the end-to-end rate through the public
-C ABI with host buffers (median of five runs, each reported), and the
+C ABI with host buffers (median of nine runs, each reported), and the
 reference's own CPU code timed on a bounded
 sample of the same workload.  Two more legs (N = 1 only):
 
@@ -51,7 +51,7 @@ from adaptflood_b200 import scenarios as sc  # noqa: E402
 
 BYTES_PER_CELL = {"f32": 28, "f64": 56}  # read H, DEM, Qx, Qy; write H', Qx', Qy'
 T_START = 1800.0
-E2E_TRIALS = 5
+E2E_TRIALS = 9
 STEPS_PER_ITERATION = 4  # step kernels per iteration of the simulation's graph loop
 
 
