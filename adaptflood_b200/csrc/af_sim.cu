@@ -235,6 +235,7 @@ struct Sim {
   cudaStream_t st = nullptr;
   af_case_desc c{};
   int P = 0, nsx = 0, nsy = 0, R = 16, WY = 4, variant = 0;
+  bool face_call = false;  // FP64: the step kernel with out-of-line faces
   size_t cells_elems = 0, qy_elems = 0;  // allocation sizes (elements, guards included)
   DevBuf H[2], Qx[2], Qy[2], DEM;
   DevBuf src_type, src_value, src_off, src_times, src_vals, src_sorted;
@@ -264,6 +265,12 @@ struct Sim {
   T* buf(DevBuf& b) const { return static_cast<T*>(b.p) + kGuard; }
 };
 
+// The step kernel of the simulation's precision, shape and face evaluation.
+static const void* step_fn(const Sim& s) {
+  return s.prec == AF_PREC_F64 ? step_kernel_f64(s.variant, s.face_call)
+                               : step_kernel_f32(s.variant);
+}
+
 static int pick_shape(Sim& s) {
   const int own = 30 * s.N;
   s.nsx = (s.c.nx + own - 1) / own;
@@ -275,7 +282,8 @@ static int pick_shape(Sim& s) {
     if (k >= 0 && k < kStepVariants) s.variant = k;
   }
   s.WY = kStepVariant[s.variant].wy;
-  const void* fn = s.prec == AF_PREC_F64 ? step_kernel_f64(s.variant) : step_kernel_f32(s.variant);
+  s.face_call = face_call_for(s.prec == AF_PREC_F64, (long long)s.c.nx * s.c.ny);
+  const void* fn = step_fn(s);
   int per_sm = 0, dev = 0, sms = kSMs;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * s.WY, 0) != cudaSuccess ||
       per_sm < 1)
@@ -478,7 +486,7 @@ static int build_graph(Sim& s) {
   // once, and the loop test runs once per iteration instead of once per step.
   void* sargs[] = {&s.prm};
   cudaKernelNodeParams ks{};
-  ks.func = const_cast<void*>(s.prec == AF_PREC_F64 ? step_kernel_f64(s.variant) : step_kernel_f32(s.variant));
+  ks.func = const_cast<void*>(step_fn(s));
   ks.gridDim = s.grid;
   ks.blockDim = s.block;
   ks.kernelParams = sargs;
@@ -712,7 +720,7 @@ static int launch(Sim& s, double t_stop, long long max_steps) {
   }
   // Host-driven fallback: launch steps in batches, checking completion.
   k_begin<<<1, 1, 0, s.st>>>(ctl, t_stop, max_steps, 0, 0);
-  const void* fn = s.prec == AF_PREC_F64 ? step_kernel_f64(s.variant) : step_kernel_f32(s.variant);
+  const void* fn = step_fn(s);
   StepParams p = s.prm;
   void* args[] = {&p};
   long long left = max_steps;

@@ -33,6 +33,7 @@
 #include <cuda_runtime.h>
 #include <cfloat>
 #include <cstdint>
+#include <cstdlib>
 
 #include "af_common.cuh"
 #include "af_pow.cuh"
@@ -262,9 +263,27 @@ __device__ inline T bc_depth(int b, SeriesTable tb, double t) {
 // `if (Q*dh < 0)` recomputation (src/kernels.cpp:86-89) yields the same Q
 // (both numerators are equal whenever Q != 0), so it is not repeated.
 
+// The FP64 wet-face expression out of line (the same results), for the step
+// kernel of mid-size grids: the four inline copies per row of a lane make the
+// row loop's code large enough to stall on instruction fetch.  Measured, ms
+// per step out of line against inline: 724^2 0.0714 / 0.0823, 1024^2 0.106 /
+// 0.124, 2048^2 0.247 / 0.269, 4096^2 0.676 / 0.716, 5793^2 1.222 / 1.265;
+// level at 512^2 (one wave of strips) and 6896^2, and on 8192^2 inline is
+// faster (2.22 against 2.32: the four faces' chains overlap in the FP64 pipe).
+static __device__ __noinline__ double face_q64(double dh, double hflow, double q0, double qa, double qb,
+                                        double qc, double qd, double dx, double gdt, double fn) {
+  const double Sf = -dh / dx;
+  const double qy_avg = (qa + qb + qc + qd) / 4.0;
+  const double qvect = sqrt(q0 * q0 + qy_avg * qy_avg);
+  const double numerator = (q0 + 0.0) - (gdt * hflow * Sf);
+  const double denominator =
+      1.0 + gdt * hflow * fn * fn * fabs(qvect) / pw::pow_ref(hflow, 10.0 / 3.0);
+  return numerator / denominator * dx;
+}
+
 // FP64: the reference's expressions exactly (src/kernels.cpp:60-84), with the
 // C library's pow algorithm (af_pow.cuh).
-template <bool ND>  // FP64 keeps every test of the reference
+template <bool ND, bool kCall = false>  // FP64 keeps every test of the reference
 __device__ inline void row_faces(const double (&h)[2], const double (&z)[2], const double (&hN)[2],
                                  const double (&zN)[2], const double (&qxo)[2],
                                  const double (&qxoN)[2], const double (&qyo)[2],
@@ -301,14 +320,19 @@ __device__ inline void row_faces(const double (&h)[2], const double (&z)[2], con
 #pragma unroll
     for (int f = 0; f < 4; f++) {
       const double dh = y0[f] - y1[f];
-      const double Sf = -dh / ph.dx;
-      const double hflow = hf[f];
-      const double qy_avg = (QA[f] + QB[f] + QC[f] + QD[f]) / 4.0;
-      const double qvect = sqrt(Q0[f] * Q0[f] + qy_avg * qy_avg);
-      const double numerator = (Q0[f] + 0.0) - (ph.gdt * hflow * Sf);
-      const double denominator =
-          1.0 + ph.gdt * hflow * ph.fn * ph.fn * fabs(qvect) / pw::pow_ref(hflow, 10.0 / 3.0);
-      const double q = numerator / denominator * ph.dx;
+      double q;
+      if constexpr (kCall) {
+        q = face_q64(dh, hf[f], Q0[f], QA[f], QB[f], QC[f], QD[f], ph.dx, ph.gdt, ph.fn);
+      } else {
+        const double Sf = -dh / ph.dx;
+        const double hflow = hf[f];
+        const double qy_avg = (QA[f] + QB[f] + QC[f] + QD[f]) / 4.0;
+        const double qvect = sqrt(Q0[f] * Q0[f] + qy_avg * qy_avg);
+        const double numerator = (Q0[f] + 0.0) - (ph.gdt * hflow * Sf);
+        const double denominator =
+            1.0 + ph.gdt * hflow * ph.fn * ph.fn * fabs(qvect) / pw::pow_ref(hflow, 10.0 / 3.0);
+        q = numerator / denominator * ph.dx;
+      }
       Q[f] = wet[f] ? q : 0.0;
     }
   }
@@ -397,7 +421,7 @@ __device__ inline float2 flux2(float2 z0, float2 h0, float2 z1, float2 h1, float
   return f2(wx ? __fdividef(num.x, den.x) : 0.0f, wy ? __fdividef(num.y, den.y) : 0.0f);
 }
 
-template <bool ND>
+template <bool ND, bool kCall = false>  // kCall: FP64 only
 __device__ inline void row_faces(const float (&h)[4], const float (&z)[4], const float (&hN)[4],
                                  const float (&zN)[4], const float (&qxo)[4],
                                  const float (&qxoN)[4], const float (&qyo)[4],
@@ -650,8 +674,9 @@ struct LaneAcc {
 // copies in flight drained and the grid's status flagged.
 // kSplitND: FP32 grids without nodata cells take a copy of the row loop
 // without the nodata tests (the same results; the batch kernel uses it, the
-// single-grid kernel measured no faster with it).
-template <typename T, bool kSplitND = false>
+// single-grid kernel measured no faster with it).  kCall: FP64 evaluates each
+// wet face out of line (see face_q64).
+template <typename T, bool kSplitND = false, bool kCall = false>
 __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>& sc, int sx,
                                           int sy, unsigned char (*ring)[4][kRowBytes],
                                           uint64_t* bar, RingPos& pos, LaneAcc<T>& acc) {
@@ -818,9 +843,10 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
     }
   }
 
-  auto rows = [&](auto edge_tag, auto nd_tag) {
+  auto rows = [&](auto edge_tag, auto nd_tag, auto call_tag) {
     constexpr bool kEdge = decltype(edge_tag)::value;
     constexpr bool kND = decltype(nd_tag)::value;
+    constexpr bool kCall = decltype(call_tag)::value;
 #pragma unroll kRowUnroll
     for (int j = j0; j < j1; j++) {
       const bool has_next = (j + 1 < ny);
@@ -859,7 +885,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
 
       // Faces of the row: interior law everywhere, then the edges.
       T qw[N], qs[N];
-      row_faces<kND>(h, z, hN, zN, qxo, qxoN, qyo, qyoN, hL, zL, qyoL, qyoNL, qxoR, qxoNR,
+      row_faces<kND, kCall>(h, z, hN, zN, qxo, qxoN, qyo, qyoN, hL, zL, qyoL, qyoNL, qxoR, qxoNR,
                      has_next, ph, qw, qs);
       if (kEdge) {
 #pragma unroll
@@ -985,12 +1011,12 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
     const bool interior = false;
 #endif
     if (nd) {
-      if (interior) rows(BoolC<false>(), BoolC<true>());
-      else rows(BoolC<true>(), BoolC<true>());
+      if (interior) rows(BoolC<false>(), BoolC<true>(), BoolC<kCall>());
+      else rows(BoolC<true>(), BoolC<true>(), BoolC<kCall>());
     } else {
-      if constexpr (sizeof(T) == 4 && kSplitND) {
-        if (interior) rows(BoolC<false>(), BoolC<false>());
-        else rows(BoolC<true>(), BoolC<false>());
+      if constexpr (kSplitND) {
+        if (interior) rows(BoolC<false>(), BoolC<false>(), BoolC<false>());
+        else rows(BoolC<true>(), BoolC<false>(), BoolC<false>());
       }
     }
   }
@@ -1052,7 +1078,7 @@ __device__ inline bool fold_step(const StepParams& p, SimCtl* ctl, double t, dou
 // Persistent grid: block b processes tiles b, b + gridDim.x, ...; a tile is
 // WY strips stacked along y (warp w owns strip sy = tile_y*WY + w of column
 // strip sx).  The last block to finish folds the step.
-template <typename T, int WY, int MINB>
+template <typename T, int WY, int MINB, bool kCall = false>
 __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
   __shared__ __align__(128) unsigned char s_ring[WY][kStages][4][kRowBytes];
   __shared__ __align__(8) uint64_t s_bar[WY][kStages];
@@ -1078,7 +1104,7 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
     const int sx = tile % p.nsx;
     const int sy = (tile / p.nsx) * WY + warp;
     if (sy >= p.nsy) continue;
-    if (!run_strip<T>(p, sc, sx, sy, s_ring[warp], bar, pos, acc)) break;
+    if (!run_strip<T, false, kCall>(p, sc, sx, sy, s_ring[warp], bar, pos, acc)) break;
   }
 
   // A valid cell's depth is finite (NaN never wins a comparison), and in
@@ -1519,6 +1545,18 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_batch_step(const BatchParams 
   if (!ok && lane == 0) atomicExch(&bp.bctl->status, 1);
 }
 
+// Whether a single grid's FP64 step takes the kernel that evaluates each wet
+// face out of line (k_step<double, ..., true>): on grids of more than 2^18
+// and at most 2^25 cells (see face_q64).  AF_SIM_FACE_CALL=0/1 forces the
+// choice (for measurements).
+constexpr long long kFaceCallMinCells = (1LL << 18) + 1;
+constexpr long long kFaceCallMaxCells = 1LL << 25;
+inline bool face_call_for(bool f64, long long cells) {
+  if (!f64) return false;
+  if (const char* v = getenv("AF_SIM_FACE_CALL")) return v[0] == '1';
+  return cells >= kFaceCallMinCells && cells <= kFaceCallMaxCells;
+}
+
 // Kernel entry points of the two precisions (defined in af_step_f64.cu and
 // af_step_f32.cu, which are compiled with different floating-point flags).
 // Launch variants: (warps per block, minimum resident blocks per SM).
@@ -1527,7 +1565,7 @@ struct StepVariant {
 };
 constexpr int kStepVariants = 5;
 constexpr StepVariant kStepVariant[kStepVariants] = {{1, 16}, {1, 12}, {1, 20}, {4, 4}, {2, 8}};
-const void* step_kernel_f64(int variant);
+const void* step_kernel_f64(int variant, bool face_call = false);
 const void* step_kernel_f32(int variant);
 const void* batch_kernel_f64(int variant);
 const void* batch_kernel_f32(int variant);

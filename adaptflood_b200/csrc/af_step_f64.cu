@@ -4,7 +4,16 @@
 
 namespace af {
 // Indices follow kStepVariant in af_step.cuh.
-const void* step_kernel_f64(int variant) {
+const void* step_kernel_f64(int variant, bool face_call) {
+  if (face_call) {
+    switch (variant) {
+      case 1: return (const void*)&k_step<double, 1, 12, true>;
+      case 2: return (const void*)&k_step<double, 1, 20, true>;
+      case 3: return (const void*)&k_step<double, 4, 4, true>;
+      case 4: return (const void*)&k_step<double, 2, 8, true>;
+      default: return (const void*)&k_step<double, 1, 16, true>;
+    }
+  }
   switch (variant) {
     case 1: return (const void*)&k_step<double, 1, 12>;
     case 2: return (const void*)&k_step<double, 1, 20>;

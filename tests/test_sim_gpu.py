@@ -25,8 +25,16 @@ FP32_DEPTH_TOL = 1e-3
 FP32_MASS_TOL = 1e-6
 
 
+# FP64 takes one of two step kernels, with the face law inline or out of line
+# (AF_SIM_FACE_CALL forces one; the default picks by grid size): both are
+# held to the same bars.
+FACE_CALL = pytest.mark.parametrize("face_call", ["0", "1"])
+
+
+@FACE_CALL
 @pytest.mark.parametrize("name", golden_names())
-def test_fused_fp64_matches_reference(cuda, name):
+def test_fused_fp64_matches_reference(cuda, name, face_call, monkeypatch):
+    monkeypatch.setenv("AF_SIM_FACE_CALL", face_call)
     case, f, exp = load_golden(name)
     with Simulation(case, "f64", forcing=f) as s:
         n = s.run(case.sim_time)
@@ -69,7 +77,9 @@ def _strip_edge_case(nx, ny, seed, R_edges=(4, 8, 16, 32), **kw):
     (250, 203, 22, dict(free=(1, 0, 1, 1), nodata_block=True, n_hvar=2)),
     (61, 300, 23, dict(free=(0, 1, 0, 1), h0=True)),
 ])
-def test_fused_fp64_matches_oracle_across_strips(cuda, nx, ny, seed, kw):
+@FACE_CALL
+def test_fused_fp64_matches_oracle_across_strips(cuda, nx, ny, seed, kw, face_call, monkeypatch):
+    monkeypatch.setenv("AF_SIM_FACE_CALL", face_call)
     case = _strip_edge_case(nx, ny, seed, **kw)
     f = fc.pack(case)
     o = orc.OracleSim(case, f)
@@ -82,6 +92,32 @@ def test_fused_fp64_matches_oracle_across_strips(cuda, nx, ny, seed, kw):
     assert np.max(np.abs(st["H"] - ref["H"])) <= DEPTH_TOL
     for k in ("Vx", "Vy"):
         assert np.max(np.abs(st[k] - ref[k])) <= VEL_TOL, k
+
+
+def test_fp64_kernels_agree_on_a_mid_size_grid(cuda, monkeypatch):
+    """A grid of 760 x 700 cells, whose default FP64 kernel has the face law
+    out of line: 150 steps equal the inline kernel's bit for bit and the
+    oracle's within 1e-9 m."""
+    case = _strip_edge_case(760, 700, 24, rain=True, n_hvar=1)
+    f = fc.pack(case)
+    out = {}
+    for mode in (None, "0"):
+        if mode is None:
+            monkeypatch.delenv("AF_SIM_FACE_CALL", raising=False)
+        else:
+            monkeypatch.setenv("AF_SIM_FACE_CALL", mode)
+        with Simulation(case, "f64", forcing=f) as s:
+            s.run(1e30, max_steps=150)
+            out[mode] = (s.status(), s.state(velocity=True))
+    assert out[None][0] == out["0"][0]
+    for k in ("H", "Qx", "Qy", "Vx", "Vy"):
+        np.testing.assert_array_equal(out[None][1][k], out["0"][1][k], err_msg=k)
+    o = orc.OracleSim(case, f)
+    o.run(1e30, max_steps=150)
+    ref = o.state(velocity=True)
+    assert np.max(np.abs(out[None][1]["H"] - ref["H"])) <= DEPTH_TOL
+    for k in ("Vx", "Vy"):
+        assert np.max(np.abs(out[None][1][k] - ref[k])) <= VEL_TOL, k
 
 
 def test_run_in_pieces_is_bit_identical(cuda):
