@@ -26,8 +26,9 @@ constexpr int kMassCap = 1 << 16;
 
 struct DevBuf {
   void* p = nullptr;
+  bool own = true;  // false: a view into another buffer's allocation
   ~DevBuf() {
-    if (p) cudaFree(p);
+    if (p && own) cudaFree(p);
   }
 };
 
@@ -236,8 +237,15 @@ struct Sim {
   af_case_desc c{};
   int P = 0, nsx = 0, nsy = 0, R = 16, WY = 4, variant = 0;
   bool face_call = false;  // FP64: the step kernel with out-of-line faces
-  size_t cells_elems = 0, qy_elems = 0;  // allocation sizes (elements, guards included)
-  DevBuf H[2], Qx[2], Qy[2], DEM;
+  bool tma = true;         // the step kernel reads rows with tiled copies
+  size_t cells_elems = 0, qy_elems = 0;  // field sizes (elements, guards included)
+  // The fields are planes of one allocation, each qy_elems long, in the order
+  // H0, DEM, Qx0, Qy0, H1, DEM (a copy), Qx1, Qy1: the four fields a step
+  // reads are then planes 4*parity .. 4*parity+3 of one 3-D tensor, which
+  // the step kernel's tiled copies (tensor map `fields`) read in one box.
+  DevBuf planes;
+  DevBuf H[2], Qx[2], Qy[2], DEM, DEM2;  // views into `planes`
+  CUtensorMap fields;
   DevBuf src_type, src_value, src_off, src_times, src_vals, src_sorted;
   DevBuf bc_type, bc_value, bc_off, bc_times, bc_vals, bc_sorted;
   DevBuf rain_times, rain_rates, spec_off, spec;
@@ -268,7 +276,7 @@ struct Sim {
 // The step kernel of the simulation's precision, shape and face evaluation.
 static const void* step_fn(const Sim& s) {
   return s.prec == AF_PREC_F64 ? step_kernel_f64(s.variant, s.face_call)
-                               : step_kernel_f32(s.variant);
+                               : step_kernel_f32(s.variant, s.tma);
 }
 
 static int pick_shape(Sim& s) {
@@ -283,6 +291,7 @@ static int pick_shape(Sim& s) {
   }
   s.WY = kStepVariant[s.variant].wy;
   s.face_call = face_call_for(s.prec == AF_PREC_F64, (long long)s.c.nx * s.c.ny);
+  s.tma = tma_for(s.prec == AF_PREC_F64, (long long)s.c.nx * s.c.ny);
   const void* fn = step_fn(s);
   int per_sm = 0, dev = 0, sms = kSMs;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * s.WY, 0) != cudaSuccess ||
@@ -334,6 +343,38 @@ static int pick_shape(Sim& s) {
   s.grid = dim3((unsigned)(tiles < slots ? tiles : slots));
   s.block = dim3(32 * s.WY);
   return AF_OK;
+}
+
+// The tensor map of the field planes: x (columns 0..nx, Qx's east face
+// included), y (rows 0..ny, Qy's last included), z (the 8 planes), from the
+// planes' first cell; a box is one 512-byte row window of 4 planes.
+static int encode_fields(Sim& s) {
+  using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeFn encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return AF_ECUDA;
+    encode = reinterpret_cast<EncodeFn>(fn);
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)s.c.nx + 1, (cuuint64_t)s.c.ny + 1, 8};
+  const cuuint64_t strides[2] = {(cuuint64_t)s.P * s.esize, (cuuint64_t)s.qy_elems * s.esize};
+  const cuuint32_t box[3] = {(cuuint32_t)(kRowBytes / s.esize), 1, 4};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  void* origin = static_cast<char*>(s.planes.p) + (size_t)kGuard * s.esize;
+  const CUresult r = encode(
+      &s.fields, s.esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+      3, origin, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+      CU_TENSOR_MAP_SWIZZLE_NONE,
+      getenv("AF_TMA_NOPROMO") ? CU_TENSOR_MAP_L2_PROMOTION_NONE : CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? AF_OK : AF_ECUDA;
 }
 
 static int alloc_field(DevBuf& b, size_t elems, int esize) {
@@ -484,7 +525,7 @@ static int build_graph(Sim& s) {
   // The loop body is kStepsPerIteration steps in a row: a step after the
   // one that ended the loop finds the control block done and returns at
   // once, and the loop test runs once per iteration instead of once per step.
-  void* sargs[] = {&s.prm};
+  void* sargs[] = {&s.prm, &s.fields};
   cudaKernelNodeParams ks{};
   ks.func = const_cast<void*>(step_fn(s));
   ks.gridDim = s.grid;
@@ -593,18 +634,20 @@ static int create(const af_case_desc* c, const af_forcing_desc* f, const double*
   const int nx = c->nx, ny = c->ny;
   s->cells_elems = cell_elems(ny, P);
   s->qy_elems = qy_elems(ny, P);
-  for (int b = 0; b < 2; b++) {
-    AF_TRY(alloc_field(s->H[b], s->cells_elems, s->esize));
-    AF_TRY(alloc_field(s->Qx[b], s->cells_elems, s->esize));
-    AF_TRY(alloc_field(s->Qy[b], s->qy_elems, s->esize));
-    AF_CUDA(cudaMemsetAsync(s->H[b].p, 0, s->cells_elems * s->esize, s->st));
-    AF_CUDA(cudaMemsetAsync(s->Qx[b].p, 0, s->cells_elems * s->esize, s->st));
-    AF_CUDA(cudaMemsetAsync(s->Qy[b].p, 0, s->qy_elems * s->esize, s->st));
+  if (const char* e = getenv("AF_PLANE_PAD")) s->qy_elems += (size_t)atoll(e);  // EXPERIMENT
+  const size_t plane_bytes = s->qy_elems * s->esize;
+  AF_TRY(alloc_field(s->planes, 8 * s->qy_elems, s->esize));
+  AF_CUDA(cudaMemsetAsync(s->planes.p, 0, 8 * plane_bytes, s->st));
+  DevBuf* order[8] = {&s->H[0], &s->DEM, &s->Qx[0], &s->Qy[0],
+                      &s->H[1], &s->DEM2, &s->Qx[1], &s->Qy[1]};
+  for (int k = 0; k < 8; k++) {
+    order[k]->p = static_cast<char*>(s->planes.p) + k * plane_bytes;
+    order[k]->own = false;
   }
-  AF_TRY(alloc_field(s->DEM, s->cells_elems, s->esize));
-  AF_CUDA(cudaMemsetAsync(s->DEM.p, 0, s->cells_elems * s->esize, s->st));
   AF_TRY(put_field(*s, s->DEM, dem, ny, nx, nx));
+  AF_CUDA(cudaMemcpyAsync(s->DEM2.p, s->DEM.p, plane_bytes, cudaMemcpyDeviceToDevice, s->st));
   if (h0) AF_TRY(put_field(*s, s->H[0], h0, ny, nx, nx));
+  AF_TRY(encode_fields(*s));
 
   HostTables tb;
   build_tables(c, f, own, s->R, s->nsx, s->nsy, tb);
@@ -722,7 +765,7 @@ static int launch(Sim& s, double t_stop, long long max_steps) {
   k_begin<<<1, 1, 0, s.st>>>(ctl, t_stop, max_steps, 0, 0);
   const void* fn = step_fn(s);
   StepParams p = s.prm;
-  void* args[] = {&p};
+  void* args[] = {&p, &s.fields};
   long long left = max_steps;
   while (left > 0) {
     long long batch = left < 64 ? left : 64;

@@ -30,6 +30,7 @@
 // loop continues (the condition of the enclosing CUDA-graph while node).
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
 #include <cuda_runtime.h>
 #include <cfloat>
 #include <cstdint>
@@ -502,6 +503,17 @@ __device__ inline void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint
       "l"(src), "r"(bytes), "r"(smem_u32(b))
       : "memory");
 }
+// One box of a 3-D tensor (TMA tiled copy, no multicast) into shared memory,
+// completing on mbarrier `b`.  `map` is the tensor map's address in kernel
+// parameter space; x * element size must be a multiple of 16 bytes.
+__device__ inline void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                   uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(b))
+      : "memory");
+}
 __device__ inline bool mbar_try_wait(uint64_t* b, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -676,10 +688,11 @@ struct LaneAcc {
 // without the nodata tests (the same results; the batch kernel uses it, the
 // single-grid kernel measured no faster with it).  kCall: FP64 evaluates each
 // wet face out of line (see face_q64).
-template <typename T, bool kSplitND = false, bool kCall = false>
+template <typename T, bool kSplitND = false, bool kCall = false, bool kTma = false>
 __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>& sc, int sx,
                                           int sy, unsigned char (*ring)[4][kRowBytes],
-                                          uint64_t* bar, RingPos& pos, LaneAcc<T>& acc) {
+                                          uint64_t* bar, RingPos& pos, LaneAcc<T>& acc,
+                                          const CUtensorMap* tmap = nullptr) {
   constexpr int N = Lanes<T>::N;
   constexpr int OWN = 30 * N;
   static_assert(32 * N * sizeof(T) == kRowBytes, "one 16-byte vector per lane");
@@ -753,12 +766,25 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
   const T* const my_src = lane == 0 ? H : lane == 1 ? Z : lane == 2 ? Qx : Qy;
   auto issue = [&](int k, int slot) {
     const int r = rfirst + k;
-    const int a_lo = r < ny ? 0 : 3;
-    const int a_hi = r < j0 ? 3 : 4;
-    if (lane == 0) mbar_expect_tx(&bar[slot], (uint32_t)(a_hi - a_lo) * row_bytes);
-    if (lane >= a_lo && lane < a_hi) {
-      fence_proxy_async();
-      bulk_g2s(&ring[slot][lane][0], my_src + (long long)r * P + wcol, row_bytes, &bar[slot]);
+    if constexpr (kTma) {
+      // One tiled copy of the row's window from all four fields: the fields
+      // are planes 4*parity .. 4*parity+3 (H, DEM, Qx, Qy) of one 3-D
+      // tensor, so the box {window, 1 row, 4 planes} lands as the stage's
+      // four 512-byte rows.  Columns past the grid (and the window's first
+      // lane on the west edge) are outside the tensor and read as zeros.
+      if (lane == 0) {
+        mbar_expect_tx(&bar[slot], 4u * kRowBytes);
+        fence_proxy_async();
+        tma_load_3d(&ring[slot][0][0], tmap, (int)wcol, r, 4 * parity, &bar[slot]);
+      }
+    } else {
+      const int a_lo = r < ny ? 0 : 3;
+      const int a_hi = r < j0 ? 3 : 4;
+      if (lane == 0) mbar_expect_tx(&bar[slot], (uint32_t)(a_hi - a_lo) * row_bytes);
+      if (lane >= a_lo && lane < a_hi) {
+        fence_proxy_async();
+        bulk_g2s(&ring[slot][lane][0], my_src + (long long)r * P + wcol, row_bytes, &bar[slot]);
+      }
     }
   };
 #endif
@@ -846,7 +872,7 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
   auto rows = [&](auto edge_tag, auto nd_tag, auto call_tag) {
     constexpr bool kEdge = decltype(edge_tag)::value;
     constexpr bool kND = decltype(nd_tag)::value;
-    constexpr bool kCall = decltype(call_tag)::value;
+    constexpr bool kFaceCall = decltype(call_tag)::value;
 #pragma unroll kRowUnroll
     for (int j = j0; j < j1; j++) {
       const bool has_next = (j + 1 < ny);
@@ -885,7 +911,8 @@ __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>
 
       // Faces of the row: interior law everywhere, then the edges.
       T qw[N], qs[N];
-      row_faces<kND, kCall>(h, z, hN, zN, qxo, qxoN, qyo, qyoN, hL, zL, qyoL, qyoNL, qxoR, qxoNR,
+      row_faces<kND, kFaceCall>(h, z, hN, zN, qxo, qxoN, qyo, qyoN, hL, zL, qyoL, qyoNL, qxoR,
+                                qxoNR,
                      has_next, ph, qw, qs);
       if (kEdge) {
 #pragma unroll
@@ -1077,9 +1104,12 @@ __device__ inline bool fold_step(const StepParams& p, SimCtl* ctl, double t, dou
 // ------------------------------------------------------- single grid
 // Persistent grid: block b processes tiles b, b + gridDim.x, ...; a tile is
 // WY strips stacked along y (warp w owns strip sy = tile_y*WY + w of column
-// strip sx).  The last block to finish folds the step.
-template <typename T, int WY, int MINB, bool kCall = false>
-__global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
+// strip sx).  The last block to finish folds the step.  kTma: rows are read
+// with one tiled copy per row through the tensor map `fields` (the grid's
+// fields as planes of one 3-D tensor); otherwise four bulk copies per row.
+template <typename T, int WY, int MINB, bool kCall = false, bool kTma = true>
+__global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p,
+                                                        const __grid_constant__ CUtensorMap fields) {
   __shared__ __align__(128) unsigned char s_ring[WY][kStages][4][kRowBytes];
   __shared__ __align__(8) uint64_t s_bar[WY][kStages];
   SimCtl* ctl = p.ctl;
@@ -1104,7 +1134,8 @@ __global__ void __launch_bounds__(32 * WY, MINB) k_step(const StepParams p) {
     const int sx = tile % p.nsx;
     const int sy = (tile / p.nsx) * WY + warp;
     if (sy >= p.nsy) continue;
-    if (!run_strip<T, false, kCall>(p, sc, sx, sy, s_ring[warp], bar, pos, acc)) break;
+    if (!run_strip<T, false, kCall, kTma>(p, sc, sx, sy, s_ring[warp], bar, pos, acc, &fields))
+      break;
   }
 
   // A valid cell's depth is finite (NaN never wins a comparison), and in
@@ -1556,6 +1587,20 @@ inline bool face_call_for(bool f64, long long cells) {
   if (const char* v = getenv("AF_SIM_FACE_CALL")) return v[0] == '1';
   return cells >= kFaceCallMinCells && cells <= kFaceCallMaxCells;
 }
+// Whether a single grid's FP32 step reads its rows with one tiled copy (TMA)
+// per row instead of four bulk copies: on grids of at most kTmaMaxCellsF32
+// cells (FP64 always).  Measured, ms per FP32 step with tiled against bulk
+// copies: 3072^2 0.0835 / 0.0868, 4096^2 0.1226 / 0.1273, 4608^2 0.1484 /
+// 0.1507; 5120^2 0.1801 / 0.1734, 5792^2 0.2262 / 0.2140, 8192^2 0.432 /
+// 0.369 (the tiled copies' DRAM reads rise with the grid, 4.7 % more bytes
+// at 6144^2).  FP64 steps are 3-4 % faster with them at every size measured
+// (1024^2 to 8192^2).  AF_SIM_TMA=0/1 forces the FP32 choice.
+constexpr long long kTmaMaxCellsF32 = 4700LL * 4700;
+inline bool tma_for(bool f64, long long cells) {
+  if (f64) return true;
+  if (const char* v = getenv("AF_SIM_TMA")) return v[0] == '1';
+  return cells <= kTmaMaxCellsF32;
+}
 
 // Kernel entry points of the two precisions (defined in af_step_f64.cu and
 // af_step_f32.cu, which are compiled with different floating-point flags).
@@ -1566,7 +1611,7 @@ struct StepVariant {
 constexpr int kStepVariants = 5;
 constexpr StepVariant kStepVariant[kStepVariants] = {{1, 16}, {1, 12}, {1, 20}, {4, 4}, {2, 8}};
 const void* step_kernel_f64(int variant, bool face_call = false);
-const void* step_kernel_f32(int variant);
+const void* step_kernel_f32(int variant, bool tma = true);
 const void* batch_kernel_f64(int variant);
 const void* batch_kernel_f32(int variant);
 // Begin and fold kernels of the batch loop (one block of kFoldThreads),

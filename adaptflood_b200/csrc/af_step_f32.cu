@@ -4,7 +4,16 @@
 
 namespace af {
 // Indices follow kStepVariant in af_step.cuh.
-const void* step_kernel_f32(int variant) {
+const void* step_kernel_f32(int variant, bool tma) {
+  if (!tma) {
+    switch (variant) {
+      case 1: return (const void*)&k_step<float, 1, 12, false, false>;
+      case 2: return (const void*)&k_step<float, 1, 20, false, false>;
+      case 3: return (const void*)&k_step<float, 4, 4, false, false>;
+      case 4: return (const void*)&k_step<float, 2, 8, false, false>;
+      default: return (const void*)&k_step<float, 1, 16, false, false>;
+    }
+  }
   switch (variant) {
     case 1: return (const void*)&k_step<float, 1, 12>;
     case 2: return (const void*)&k_step<float, 1, 20>;
