@@ -275,7 +275,7 @@ struct Sim {
 
 // The step kernel of the simulation's precision, shape and face evaluation.
 static const void* step_fn(const Sim& s) {
-  return s.prec == AF_PREC_F64 ? step_kernel_f64(s.variant, s.face_call)
+  return s.prec == AF_PREC_F64 ? step_kernel_f64(s.variant, s.face_call, s.tma)
                                : step_kernel_f32(s.variant, s.tma);
 }
 

@@ -1587,19 +1587,23 @@ inline bool face_call_for(bool f64, long long cells) {
   if (const char* v = getenv("AF_SIM_FACE_CALL")) return v[0] == '1';
   return cells >= kFaceCallMinCells && cells <= kFaceCallMaxCells;
 }
-// Whether a single grid's FP32 step reads its rows with one tiled copy (TMA)
-// per row instead of four bulk copies: on grids of at most kTmaMaxCellsF32
-// cells (FP64 always).  Measured, ms per FP32 step with tiled against bulk
-// copies: 3072^2 0.0835 / 0.0868, 4096^2 0.1226 / 0.1273, 4608^2 0.1484 /
-// 0.1507; 5120^2 0.1801 / 0.1734, 5792^2 0.2262 / 0.2140, 8192^2 0.432 /
-// 0.369 (the tiled copies' DRAM reads rise with the grid, 4.7 % more bytes
-// at 6144^2).  FP64 steps are 3-4 % faster with them at every size measured
-// (1024^2 to 8192^2).  AF_SIM_TMA=0/1 forces the FP32 choice.
+// Whether a single grid's step reads its rows with one tiled copy (TMA) per
+// row instead of four bulk copies: FP32 grids of at most kTmaMaxCellsF32
+// cells, FP64 grids of at most kTmaMaxCellsF64.  The tiled copies take fewer
+// instructions but read a few per cent more DRAM bytes, so they pay where the
+// step is bound by issue or latency and lose where it is bound by bandwidth.
+// Measured, ms per FP32 step with tiled against bulk copies: 3072^2 0.0835 /
+// 0.0868, 4096^2 0.1226 / 0.1273, 4608^2 0.1484 / 0.1507; 5120^2 0.1801 /
+// 0.1734, 5792^2 0.2262 / 0.2140, 8192^2 0.432 / 0.369.  FP64, wet grids:
+// 3-5 % faster at every size from 1024^2 to 16384^2 (8192^2 2.12 against
+// 2.21 ms), but 6 % slower on the mostly dry 16384^2 start of the ponds
+// configuration, where the FP64 step is bandwidth-bound too.
+// AF_SIM_TMA=0/1 forces the choice.
 constexpr long long kTmaMaxCellsF32 = 4700LL * 4700;
+constexpr long long kTmaMaxCellsF64 = 1LL << 26;
 inline bool tma_for(bool f64, long long cells) {
-  if (f64) return true;
   if (const char* v = getenv("AF_SIM_TMA")) return v[0] == '1';
-  return cells <= kTmaMaxCellsF32;
+  return cells <= (f64 ? kTmaMaxCellsF64 : kTmaMaxCellsF32);
 }
 
 // Kernel entry points of the two precisions (defined in af_step_f64.cu and
@@ -1610,7 +1614,7 @@ struct StepVariant {
 };
 constexpr int kStepVariants = 5;
 constexpr StepVariant kStepVariant[kStepVariants] = {{1, 16}, {1, 12}, {1, 20}, {4, 4}, {2, 8}};
-const void* step_kernel_f64(int variant, bool face_call = false);
+const void* step_kernel_f64(int variant, bool face_call = false, bool tma = true);
 const void* step_kernel_f32(int variant, bool tma = true);
 const void* batch_kernel_f64(int variant);
 const void* batch_kernel_f32(int variant);

@@ -4,7 +4,16 @@
 
 namespace af {
 // Indices follow kStepVariant in af_step.cuh.
-const void* step_kernel_f64(int variant, bool face_call) {
+const void* step_kernel_f64(int variant, bool face_call, bool tma) {
+  if (!tma) {  // large grids: the face law inline, bulk copies
+    switch (variant) {
+      case 1: return (const void*)&k_step<double, 1, 12, false, false>;
+      case 2: return (const void*)&k_step<double, 1, 20, false, false>;
+      case 3: return (const void*)&k_step<double, 4, 4, false, false>;
+      case 4: return (const void*)&k_step<double, 2, 8, false, false>;
+      default: return (const void*)&k_step<double, 1, 16, false, false>;
+    }
+  }
   if (face_call) {
     switch (variant) {
       case 1: return (const void*)&k_step<double, 1, 12, true>;
