@@ -345,36 +345,11 @@ static int pick_shape(Sim& s) {
   return AF_OK;
 }
 
-// The tensor map of the field planes: x (columns 0..nx, Qx's east face
-// included), y (rows 0..ny, Qy's last included), z (the 8 planes), from the
-// planes' first cell; a box is one 512-byte row window of 4 planes.
+// The tensor map of the field planes (see encode_field_planes).
 static int encode_fields(Sim& s) {
-  using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-  static EncodeFn encode = nullptr;
-  if (!encode) {
-    void* fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
-            cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !fn)
-      return AF_ECUDA;
-    encode = reinterpret_cast<EncodeFn>(fn);
-  }
-  const cuuint64_t dims[3] = {(cuuint64_t)s.c.nx + 1, (cuuint64_t)s.c.ny + 1, 8};
-  const cuuint64_t strides[2] = {(cuuint64_t)s.P * s.esize, (cuuint64_t)s.qy_elems * s.esize};
-  const cuuint32_t box[3] = {(cuuint32_t)(kRowBytes / s.esize), 1, 4};
-  const cuuint32_t estr[3] = {1, 1, 1};
   void* origin = static_cast<char*>(s.planes.p) + (size_t)kGuard * s.esize;
-  const CUresult r = encode(
-      &s.fields, s.esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-      3, origin, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-      CU_TENSOR_MAP_SWIZZLE_NONE,
-      getenv("AF_TMA_NOPROMO") ? CU_TENSOR_MAP_L2_PROMOTION_NONE : CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return r == CUDA_SUCCESS ? AF_OK : AF_ECUDA;
+  return encode_field_planes(&s.fields, origin, s.esize, s.c.nx, s.c.ny, s.P,
+                             s.qy_elems * s.esize);
 }
 
 static int alloc_field(DevBuf& b, size_t elems, int esize) {

@@ -688,6 +688,7 @@ struct LaneAcc {
 // without the nodata tests (the same results; the batch kernel uses it, the
 // single-grid kernel measured no faster with it).  kCall: FP64 evaluates each
 // wet face out of line (see face_q64).
+// kTma: one tiled copy per row through `tmap` instead of four bulk copies.
 template <typename T, bool kSplitND = false, bool kCall = false, bool kTma = false>
 __device__ __forceinline__ bool run_strip(const StepParams& p, const StepScal<T>& sc, int sx,
                                           int sy, unsigned char (*ring)[4][kRowBytes],
@@ -1604,6 +1605,38 @@ constexpr long long kTmaMaxCellsF64 = 1LL << 26;
 inline bool tma_for(bool f64, long long cells) {
   if (const char* v = getenv("AF_SIM_TMA")) return v[0] == '1';
   return cells <= (f64 ? kTmaMaxCellsF64 : kTmaMaxCellsF32);
+}
+
+// The tensor map of a grid's field planes: 8 planes (H0, DEM, Qx0, Qy0, H1,
+// DEM, Qx1, Qy1) `plane_bytes` apart from `origin` (the first plane's cell
+// (0, 0)), rows P elements apart; x covers columns 0..nx (Qx's east face
+// included), y rows 0..ny (Qy's last included), z the planes; a box is one
+// 512-byte row window of 4 planes.  AF_ECUDA if the driver refuses it.
+inline int encode_field_planes(CUtensorMap* out, void* origin, int esize, int nx, int ny, int P,
+                               size_t plane_bytes) {
+  using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeFn encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return AF_ECUDA;
+    encode = reinterpret_cast<EncodeFn>(fn);
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)nx + 1, (cuuint64_t)ny + 1, 8};
+  const cuuint64_t strides[2] = {(cuuint64_t)P * esize, (cuuint64_t)plane_bytes};
+  const cuuint32_t box[3] = {(cuuint32_t)(kRowBytes / esize), 1, 4};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = encode(
+      out, esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+      origin, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? AF_OK : AF_ECUDA;
 }
 
 // Kernel entry points of the two precisions (defined in af_step_f64.cu and
