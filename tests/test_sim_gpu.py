@@ -120,6 +120,27 @@ def test_fp64_kernels_agree_on_a_mid_size_grid(cuda, monkeypatch):
         assert np.max(np.abs(out[None][1][k] - ref[k])) <= VEL_TOL, k
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_row_copy_methods_agree(cuda, prec, monkeypatch):
+    """The step reads its rows with one tiled copy per row (small and mid-size
+    grids) or four bulk copies (large grids; AF_SIM_TMA forces either): the
+    same states bit for bit, here on a case with sources and depth BCs on
+    strip edges, nodata and a grid width that ends mid-strip."""
+    case = _strip_edge_case(250, 203, 25, free=(1, 0, 1, 1), nodata_block=True, n_hvar=2)
+    f = fc.pack(case)
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("AF_SIM_TMA", mode)
+        with Simulation(case, prec, forcing=f) as s:
+            s.run(case.sim_time)
+            out[mode] = (s.status(), s.state(velocity=True), s.mass_series())
+    assert out["0"][0] == out["1"][0]
+    for k in ("H", "Qx", "Qy", "Vx", "Vy"):
+        np.testing.assert_array_equal(out["0"][1][k], out["1"][1][k], err_msg=k)
+    for a, b in zip(out["0"][2], out["1"][2]):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_run_in_pieces_is_bit_identical(cuda):
     case, f, exp = load_golden("closed_rain_points")
     with Simulation(case, "f64", forcing=f) as a, Simulation(case, "f64", forcing=f) as b:
