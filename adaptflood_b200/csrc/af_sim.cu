@@ -322,6 +322,12 @@ static int pick_shape(Sim& s) {
     if (cells <= (1LL << 20)) s.R = 2;
     else if (cells <= (1LL << 23)) s.R = 8;
     else if (cells <= (1LL << 25)) s.R = 16;
+  } else if (cells < (1LL << 20)) {
+    // Small FP32 grids: one-row strips, the shortest chain per warp even at
+    // slightly over one wave (ms per step, one row against the two-wave rule:
+    // 512^2 0.0312 / 0.0369, 724^2 0.0372 / 0.0393; at 1024^2 and above the
+    // rule is as fast or faster).
+    s.R = 1;
   } else {
     const long long waves = (tiles_for(32) + slots - 1) / slots;
     if (waves <= 2) {
